@@ -1,0 +1,142 @@
+// ref_driver.cc -- a driver around the UNMODIFIED reference CPU code
+// (RDMCE src/graph.cc, src/mce.cc, src/common.cu), compiled out-of-tree by
+// oracle/Makefile into oracle/_ref/ref_cpu.  Test infrastructure only: it pins
+// the oracle (loader conventions, degeneracy value, clique counts) and is the
+// "reference" CPU baseline that bench.py --impl reference times.
+//
+// Modes:
+//   ref_cpu count <graph>            MceSolver::Solve(BKFixedMemPivotBit), 1 thread
+//   ref_cpu pivot <graph>            MceSolver::Solve(BKPivot), 1 thread
+//   ref_cpu par <graph> <threads> [max_roots]
+//                                    root-parallel: one MceSolver per thread, the
+//                                    vertex roots of src/mce.cc:66-95 handed out in
+//                                    chunks, each solved by BKFixedMemPivotBit2
+//   ref_cpu stats <graph>            n, m, max degree, degeneracy after the sort
+//   ref_cpu csr <graph> <out>        CSR + labels after the sort (binary dump)
+// <graph> is COO text (sorted by degeneracy as main.cc:26-27 does) or a .bin.
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <functional>
+#include <iostream>
+#include <string>
+#include <thread>
+#include <vector>
+#include <algorithm>
+#include <memory>
+#include <sstream>
+#include <unordered_map>
+#include <queue>
+#include <cassert>
+#include <limits>
+// The per-root solver entry points are private members of MceSolver; the
+// root-parallel harness needs them, so open the class for this driver only.
+#define private public
+#include "mce.h"
+#undef private
+
+static void load(Graph &g, const std::string &path) {
+  if (path.size() >= 4 && path.substr(path.size() - 4) == ".bin") {
+    g.LoadFromBin(path);
+  } else {
+    g.LoadFromFile(path);
+    g.SortByOrder(OrderType::DEG);
+  }
+}
+
+int main(int argc, char **argv) {
+  if (argc < 3) {
+    std::fprintf(stderr, "usage: %s count|pivot|par|stats|csr <graph> [...]\n", argv[0]);
+    return 2;
+  }
+  std::string mode = argv[1];
+  Graph g;
+  load(g, argv[2]);
+  if (mode == "stats") {
+    std::printf("n %zu m %zu max_degree %zu degeneracy %zu\n", g.GetNumVertices(), g.GetNumEdges(),
+                g.GetMaxDegree(), g.GetDegeneracy());
+    return 0;
+  }
+  if (mode == "csr") {
+    if (argc < 4) return 2;
+    g.ConvertToCsr();
+    FILE *f = std::fopen(argv[3], "wb");
+    if (!f) return 1;
+    uint64_t n = g.GetNumVertices(), m = g.GetNumEdges();
+    std::fwrite(&n, 8, 1, f);
+    std::fwrite(&m, 8, 1, f);
+    std::fwrite(g.GetRowOffset(), 4, n + 1, f);
+    std::fwrite(g.GetColIdx(), 4, 2 * m, f);
+    // labels are not exposed by Graph; recover them through the operator<< dump
+    std::ostringstream os;
+    os << g;
+    std::istringstream is(os.str());
+    std::string line;
+    std::vector<uint32_t> labels(n, 0);
+    while (std::getline(is, line)) {
+      if (line.size() < 2 || line[0] != 'v') continue;
+      unsigned long id = 0, lab = 0;
+      if (std::sscanf(line.c_str(), "v%lu(%lu)", &id, &lab) == 2 && id < n) labels[id] = (uint32_t)lab;
+    }
+    std::fwrite(labels.data(), 4, n, f);
+    std::fclose(f);
+    return 0;
+  }
+  if (mode == "count" || mode == "pivot") {
+    MceSolver s(g);
+    auto t0 = std::chrono::steady_clock::now();
+    s.Solve(mode == "count" ? MceAlgorithm::BKFixedMemPivotBit : MceAlgorithm::BKPivot);
+    double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::printf("RESULT count %llu seconds %.6f threads 1\n", (unsigned long long)s.mce_count_, sec);
+    return 0;
+  }
+  if (mode == "par") {
+    int threads = argc > 3 ? std::atoi(argv[3]) : (int)std::thread::hardware_concurrency();
+    if (threads < 1) threads = 1;
+    uint64_t n = g.GetNumVertices();
+    uint64_t limit = argc > 4 ? std::strtoull(argv[4], nullptr, 10) : n;
+    if (limit > n) limit = n;
+    std::atomic<uint64_t> next(0);
+    std::vector<uint64_t> counts(threads, 0);
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> th;
+    for (int t = 0; t < threads; t++) {
+      th.emplace_back([&, t]() {
+        MceSolver s(g);
+        for (;;) {
+          uint64_t k0 = next.fetch_add(16);
+          if (k0 >= limit) break;
+          uint64_t k1 = std::min(limit, k0 + 16);
+          for (uint64_t k = k0; k < k1; k++) {
+            // heavy (late) vertices first, as the GPU kernel orders its roots
+            vid_t v0 = (vid_t)(n - 1 - k);
+            vlist_t R, P, X;
+            R.emplace_back(v0);
+            for (vid_t v1 : g.N(v0)) {
+              if (v0 > v1) X.emplace_back(v1);
+              else P.emplace_back(v1);
+            }
+            if (P.empty()) {
+              if (X.empty()) s.IncrementMceCount();
+              continue;
+            }
+            s.BKFixedMemPivotBit2(R, P, X);
+          }
+        }
+        counts[t] = s.mce_count_;
+      });
+    }
+    for (auto &x : th) x.join();
+    double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    uint64_t total = 0;
+    for (auto c : counts) total += c;
+    std::printf("RESULT count %llu seconds %.6f threads %d roots %llu\n", (unsigned long long)total, sec,
+                threads, (unsigned long long)limit);
+    return 0;
+  }
+  std::fprintf(stderr, "unknown mode %s\n", mode.c_str());
+  return 2;
+}

@@ -1,0 +1,125 @@
+// engine.h -- device-resident graph and the entry points of the GPU pipeline.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace mce {
+
+// A degeneracy-ordered graph resident in HBM (the role of GraphGpu,
+// include/graph_gpu.cuh:5-57, plus the root list and label hashes).
+struct DeviceGraph {
+  uint32_t n = 0;
+  uint64_t m = 0;
+  uint32_t *off = nullptr;      // n + 1
+  uint32_t *adj = nullptr;      // 2m
+  uint32_t *labels = nullptr;   // n
+  uint64_t *h1 = nullptr;       // n
+  uint64_t *h2 = nullptr;       // n
+  uint32_t *root_v0 = nullptr;  // m
+  uint32_t *root_v1 = nullptr;  // m
+  uint32_t *slot = nullptr;     // n, batched mode only
+  uint32_t max_degree = 0;
+  uint32_t degeneracy = 0;
+  cudaStream_t stream = nullptr;
+};
+
+mce_status build_from_pairs(const uint32_t *u_d, const uint32_t *v_d, uint64_t np, int order_kind,
+                            uint64_t spin_limit, cudaStream_t st, DeviceGraph *g);
+mce_status finish_graph(uint32_t n, uint64_t m, const uint32_t *eu, const uint32_t *ev, const uint32_t *deg,
+                        const uint32_t *labels0, int order_kind, uint64_t spin_limit, cudaStream_t st,
+                        DeviceGraph *g);
+mce_status build_from_csr(uint64_t n, const uint32_t *off_d, const uint32_t *adj_d, const uint32_t *labels_d,
+                          int already_ordered, int order_kind, uint32_t degeneracy_hint, uint64_t spin_limit,
+                          cudaStream_t st, DeviceGraph *g);
+mce_status csr_to_edges(uint64_t n, const uint32_t *off, const uint32_t *adj, uint64_t m, uint32_t *deg,
+                        uint32_t **eu, uint32_t **ev, cudaStream_t st);
+void free_graph(DeviceGraph *g);
+
+struct EnumConfig {
+  uint32_t warps_per_block = 0;
+  uint32_t blocks_per_sm = 0;
+  uint32_t share_bound = 24;
+  int expand_r = 1;
+  int sharing = 1;
+  uint64_t root_begin = 0, root_end = 0;
+  uint64_t spin_limit = 0;
+  const uint64_t *root_list = nullptr;  // device: explicit root ids (per-root mode)
+  uint64_t n_root_list = 0;
+  unsigned long long *per_root_count = nullptr;     // device, n_root_list
+  unsigned long long *per_root_checksum = nullptr;  // device, n_root_list
+  uint32_t n_slots = 1;
+  uint32_t hist_len = MCE_HIST_LEN;
+  uint32_t max_blocks = 0;  // cap on the grid (0 = whole GPU); the server shares the GPU
+};
+
+struct EnumStats {
+  uint64_t roots = 0;
+  uint64_t heavy_roots = 0;
+  uint64_t shared_tasks = 0;
+  uint32_t error = 0;
+  float ms_setup = 0, ms_enum = 0;
+  uint64_t launches = 0;
+};
+
+// Per-slot results written by the enumeration kernels.
+struct SlotResult {
+  unsigned long long count;
+  unsigned long long checksum;
+  unsigned int max_size;
+  unsigned int pad;
+};
+
+struct Scratch;
+
+// Kernel parameters of one enumeration launch.
+struct EnumParams {
+  DevGraph g;
+  uint64_t rb, re;                       // root range [rb, re) (range mode)
+  const uint32_t *heavy_list;            // heavy pass: root ids
+  const uint64_t *root_list;             // per-root mode: root ids
+  uint64_t n_list;                       // entries in whichever list is used
+  unsigned long long *next;              // claim counter
+  char *slab;
+  uint64_t slab_bytes;                   // per warp
+  uint32_t *heavy_out;                   // range mode: deferred roots
+  unsigned int *heavy_n;
+  unsigned long long *heavy_need;
+  int push_heavy;
+  SlotResult *slots;
+  unsigned long long *hist;
+  uint32_t hist_len;
+  unsigned long long *per_root_count;
+  unsigned long long *per_root_checksum;
+  int expand_r;
+  unsigned int *error;
+  unsigned long long *stat_roots;
+};
+
+
+// A planned enumeration: scratch allocated, launch shape fixed.  Launch may be
+// captured into a CUDA graph; finish reads the control words and runs the
+// large-scratch pass for deferred roots.
+struct EnumPlan {
+  EnumParams params{};
+  uint32_t blocks = 0, threads = 0;
+  size_t smem = 0;
+  uint64_t nwarps = 0, nwork = 0;
+  bool fits_all = false;  // every root fits the normal slab: no deferred pass possible
+  void *ctl = nullptr;
+  Scratch *scr = nullptr;
+};
+
+// Enumerate; results accumulate into slots[n_slots] and hist[n_slots * hist_len]
+// (device buffers the caller zeroed).
+mce_status enumerate(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, cudaStream_t st, SlotResult *slots,
+                     unsigned long long *hist, EnumStats *stats);
+mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, SlotResult *slots,
+                     unsigned long long *hist, EnumPlan *plan);
+mce_status enum_launch(const EnumPlan &plan, cudaStream_t st);
+mce_status enum_finish(const EnumPlan &plan, cudaStream_t st, EnumStats *stats);
+
+}  // namespace mce

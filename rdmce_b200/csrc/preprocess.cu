@@ -1,0 +1,589 @@
+// preprocess.cu -- COO pairs -> degeneracy-ordered CSR, entirely on the GPU.
+//
+// Replaces the reference's single-threaded host pipeline:
+//   Graph::LoadFromFile edge handling   src/graph.cc:140-204  (self-loops dropped,
+//       u<v, sort+unique, dense relabel of present labels in ascending order)
+//   Graph::SortByDegeneracy/ApplyOrder  src/graph.cc:333-358, 54-77
+//   Graph::ConvertToCsr + LoadFromCpu   src/graph.cc:268-288, src/graph_gpu.cu:3-58
+// Steps: pack (min,max) keys -> radix sort -> unique -> mark/scan dense ids ->
+// degrees -> level-synchronous k-core peeling (one persistent launch per level,
+// cascade through a device queue) -> relabel both edge directions -> radix sort
+// -> CSR offsets by scan -> root list (v0 < v1) by flag+scan.
+// The peel order inside a level differs from the reference's scan+BFS order;
+// any peeling order gives the same degeneracy value and the same clique set.
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+#include "engine.h"
+
+namespace mce {
+
+namespace {
+
+constexpr uint64_t kInvalidKey = ~0ULL;
+
+__global__ void k_pack_keys(const uint32_t *u, const uint32_t *v, uint64_t n, int bits, uint64_t *keys) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t a = u[i], b = v[i];
+    if (a == b) {
+      keys[i] = kInvalidKey;
+      continue;
+    }
+    if (a > b) {
+      uint32_t t = a;
+      a = b;
+      b = t;
+    }
+    keys[i] = ((uint64_t)a << bits) | b;
+  }
+}
+
+__global__ void k_unique_flags(const uint64_t *keys, uint64_t n, uint32_t *flags) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t k = keys[i];
+    flags[i] = (k != kInvalidKey && (i == 0 || keys[i - 1] != k)) ? 1u : 0u;
+  }
+}
+
+__global__ void k_compact_keys(const uint64_t *keys, const uint32_t *flags, const uint32_t *pos, uint64_t n,
+                               uint64_t *out) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    if (flags[i]) out[pos[i]] = keys[i];
+}
+
+__global__ void k_mark_labels(const uint64_t *edges, uint64_t m, int bits, uint32_t *mark) {
+  const uint64_t mask = (1ULL << bits) - 1;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+    mark[edges[i] >> bits] = 1;
+    mark[edges[i] & mask] = 1;
+  }
+}
+
+__global__ void k_labels_from_marks(const uint32_t *mark, const uint32_t *id, uint64_t nl, uint32_t *labels) {
+  for (uint64_t l = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; l < nl; l += (uint64_t)gridDim.x * blockDim.x)
+    if (mark[l]) labels[id[l]] = (uint32_t)l;
+}
+
+// edges (label pair) -> dense ids, degrees
+__global__ void k_map_edges(uint64_t *edges, uint64_t m, int bits, const uint32_t *id, uint32_t *eu,
+                            uint32_t *ev, uint32_t *deg) {
+  const uint64_t mask = (1ULL << bits) - 1;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t a = id[edges[i] >> bits], b = id[edges[i] & mask];
+    eu[i] = a;
+    ev[i] = b;
+    atomicAdd(&deg[a], 1u);
+    atomicAdd(&deg[b], 1u);
+  }
+}
+
+// unsorted symmetric adjacency for peeling
+__global__ void k_fill_adj(const uint32_t *eu, const uint32_t *ev, uint64_t m, uint32_t *cursor, uint32_t *adj) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t a = eu[i], b = ev[i];
+    adj[atomicAdd(&cursor[a], 1u)] = b;
+    adj[atomicAdd(&cursor[b], 1u)] = a;
+  }
+}
+
+__global__ void k_iota(uint32_t *a, uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    a[i] = (uint32_t)i;
+}
+
+// ---- k-core peeling: one persistent launch per level k ----
+struct PeelCtl {
+  uint32_t tail;       // entries appended to order[]
+  uint32_t head;       // next order[] entry to take
+  uint32_t processed;  // entries whose neighbours were decremented
+  uint32_t scan_done;  // warps finished with the level scan
+  uint32_t next_n;     // survivors appended to the next remaining list
+  uint32_t min_rest;   // smallest degree > k seen among unclaimed vertices
+  uint32_t claimed;    // claims at this level
+  uint32_t error;      // nonzero: a bounded wait expired
+};
+
+__device__ __forceinline__ void peel_claim(uint32_t v, uint32_t *state, uint32_t *order, PeelCtl *ctl) {
+  if (atomicCAS(&state[v], 0u, 1u) == 0u) {
+    uint32_t p = atomicAdd(&ctl->tail, 1u);
+    atomicAdd(&ctl->claimed, 1u);
+    volatile uint32_t *o = order;
+    o[p] = v;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_peel_level(uint32_t k, const uint32_t *rem, uint32_t nrem,
+                                                    uint32_t *rem_next, const uint32_t *off,
+                                                    const uint32_t *adj, int *deg, uint32_t *state,
+                                                    uint32_t *order, PeelCtl *ctl, uint32_t total_warps,
+                                                    uint64_t spin_limit) {
+  const uint32_t lane = lane_id();
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  // 1) scan the remaining vertices: claim degree <= k, keep the rest
+  uint32_t local_min = 0xffffffffu;
+  for (uint32_t i = gwarp * 32 + lane; i < nrem; i += total_warps * 32) {
+    uint32_t v = rem[i];
+    if (state[v] != 0) continue;
+    int d = deg[v];
+    if (d <= (int)k) {
+      peel_claim(v, state, order, ctl);
+    } else {
+      rem_next[atomicAdd(&ctl->next_n, 1u)] = v;
+      local_min = min(local_min, (uint32_t)d);
+    }
+  }
+  local_min = __reduce_min_sync(kFull, local_min);
+  if (lane == 0) {
+    if (local_min != 0xffffffffu) atomicMin(&ctl->min_rest, local_min);
+    __threadfence();
+    atomicAdd(&ctl->scan_done, 1u);
+  }
+  // 2) cascade: process claimed vertices through the order[] queue
+  volatile PeelCtl *vc = ctl;
+  volatile uint32_t *vorder = order;
+  uint64_t spins = 0;
+  for (;;) {
+    uint32_t idx = 0;
+    if (lane == 0) idx = atomicAdd(&ctl->head, 1u);
+    idx = __shfl_sync(kFull, idx, 0);
+    // wait until idx is claimed, or the level is finished
+    bool have = false;
+    for (;;) {
+      uint32_t t = 0, done = 0, sd = 0;
+      if (lane == 0) {
+        // order matters: scans finished, then processed, then tail.  processed
+        // never exceeds tail, so processed == tail read in this order means no
+        // entry was in flight and no claim can follow.
+        sd = vc->scan_done;
+        __threadfence();
+        done = vc->processed;
+        __threadfence();
+        t = vc->tail;
+      }
+      t = __shfl_sync(kFull, t, 0);
+      sd = __shfl_sync(kFull, sd, 0);
+      done = __shfl_sync(kFull, done, 0);
+      if (idx < t) {
+        have = true;
+        break;
+      }
+      if (sd == total_warps && done == t) break;  // no claim can arrive any more
+      if (++spins > spin_limit) {
+        if (lane == 0) atomicExch(&ctl->error, 1u);
+        return;
+      }
+      __nanosleep(200);
+    }
+    if (!have) return;
+    uint32_t v = 0xffffffffu;
+    if (lane == 0) {
+      while ((v = vorder[idx]) == 0xffffffffu) {
+        if (++spins > spin_limit) {
+          atomicExch(&ctl->error, 1u);
+          break;
+        }
+      }
+    }
+    v = __shfl_sync(kFull, v, 0);
+    if (v == 0xffffffffu) return;
+    for (uint32_t e = off[v] + lane; e < off[v + 1]; e += 32) {
+      uint32_t u = adj[e];
+      if (state[u] != 0) continue;
+      int old = atomicSub(&deg[u], 1);
+      if (old == (int)k + 1) peel_claim(u, state, order, ctl);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence();
+      atomicAdd(&ctl->processed, 1u);
+    }
+  }
+}
+
+__global__ void k_rank_from_order(const uint32_t *order, uint32_t n, uint32_t *rank) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) rank[order[i]] = i;
+}
+
+// both directions of every edge under the new ids, packed (row << nb) | col
+__global__ void k_relabel_keys(const uint32_t *eu, const uint32_t *ev, uint64_t m, const uint32_t *rank, int nb,
+                               uint64_t *keys, uint32_t *deg_new) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t a = rank[eu[i]], b = rank[ev[i]];
+    keys[2 * i] = ((uint64_t)a << nb) | b;
+    keys[2 * i + 1] = ((uint64_t)b << nb) | a;
+    atomicAdd(&deg_new[a], 1u);
+    atomicAdd(&deg_new[b], 1u);
+  }
+}
+
+__global__ void k_csr_cols(const uint64_t *keys, uint64_t m2, int nb, uint32_t *adj, uint32_t *upflag) {
+  const uint64_t mask = (1ULL << nb) - 1;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m2; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t r = (uint32_t)(keys[i] >> nb), c = (uint32_t)(keys[i] & mask);
+    adj[i] = c;
+    upflag[i] = r < c ? 1u : 0u;
+  }
+}
+
+__global__ void k_roots(const uint64_t *keys, uint64_t m2, int nb, const uint32_t *upflag, const uint32_t *pos,
+                        uint32_t *root_v0, uint32_t *root_v1) {
+  const uint64_t mask = (1ULL << nb) - 1;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m2; i += (uint64_t)gridDim.x * blockDim.x)
+    if (upflag[i]) {
+      root_v0[pos[i]] = (uint32_t)(keys[i] >> nb);
+      root_v1[pos[i]] = (uint32_t)(keys[i] & mask);
+    }
+}
+
+__global__ void k_permute_labels(const uint32_t *labels_old, const uint32_t *rank, uint32_t n, uint32_t *labels,
+                                 uint64_t *h1, uint64_t *h2) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t l = labels_old[i];
+    uint32_t r = rank ? rank[i] : i;
+    labels[r] = l;
+    h1[r] = mix64((uint64_t)l);
+    h2[r] = mix64((uint64_t)l ^ kGolden);
+  }
+}
+
+__global__ void k_degree_keys(const uint32_t *deg, uint32_t n, int desc, uint64_t *keys) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t d = desc ? ~deg[i] : deg[i];
+    keys[i] = ((uint64_t)d << 32) | i;
+  }
+}
+
+__global__ void k_order_from_keys(const uint64_t *keys, uint32_t n, uint32_t *order) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    order[i] = (uint32_t)keys[i];
+}
+
+int bits_for(uint64_t maxval) {
+  int b = 1;
+  while (b < 64 && (maxval >> b) != 0) b++;
+  return b;
+}
+
+template <typename T>
+struct DevBuf {
+  T *p = nullptr;
+  cudaStream_t st = nullptr;
+  mce_status alloc(size_t n, cudaStream_t s) {
+    st = s;
+    if (cudaMallocAsync(&p, std::max<size_t>(n, 1) * sizeof(T), s) != cudaSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+      return MCE_ERR_OUT_OF_MEMORY;
+    }
+    return MCE_OK;
+  }
+  void release() {
+    if (p) cudaFreeAsync(p, st);
+    p = nullptr;
+  }
+  ~DevBuf() { release(); }
+};
+
+template <typename T>
+mce_status read_scalar(const T *d, T *h, cudaStream_t st) {
+  MCE_CUDA_TRY(cudaMemcpyAsync(h, d, sizeof(T), cudaMemcpyDeviceToHost, st));
+  MCE_CUDA_TRY(cudaStreamSynchronize(st));
+  return MCE_OK;
+}
+
+// k-core peeling over an unsorted symmetric CSR; fills order[] (position -> vertex)
+mce_status peel(uint32_t n, const uint32_t *off, const uint32_t *adj, const uint32_t *deg0, uint32_t *order,
+                uint32_t *degeneracy, uint64_t spin_limit, cudaStream_t st) {
+  DevBuf<int> deg;
+  DevBuf<uint32_t> state, remA, remB;
+  DevBuf<PeelCtl> ctl;
+  MCE_TRY(deg.alloc(n, st));
+  MCE_TRY(state.alloc(n, st));
+  MCE_TRY(remA.alloc(n, st));
+  MCE_TRY(remB.alloc(n, st));
+  MCE_TRY(ctl.alloc(1, st));
+  MCE_CUDA_TRY(cudaMemcpyAsync(deg.p, deg0, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+  MCE_CUDA_TRY(cudaMemsetAsync(state.p, 0, n * sizeof(uint32_t), st));
+  MCE_CUDA_TRY(cudaMemsetAsync(order, 0xff, n * sizeof(uint32_t), st));
+  k_iota<<<grid_for(n, 256), 256, 0, st>>>(remA.p, n);
+  int dev = 0;
+  MCE_CUDA_TRY(cudaGetDevice(&dev));
+  int sms = 0, per_sm = 0;
+  MCE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  MCE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel_level, 256, 0));
+  // every block must be resident: waiting warps spin on work other warps produce
+  uint32_t blocks = (uint32_t)std::max(1, std::min(per_sm, 4)) * (uint32_t)sms;
+  uint32_t total_warps = blocks * 8;
+  PeelCtl h{};
+  uint32_t nrem = n, tail = 0, k = 0, degen = 0;
+  PeelCtl *hc = nullptr;
+  MCE_CUDA_TRY(cudaMallocHost(&hc, sizeof(PeelCtl)));
+  mce_status s = MCE_OK;
+  while (tail < n) {
+    h = PeelCtl{};
+    h.tail = tail;
+    h.head = tail;
+    h.processed = tail;
+    h.min_rest = 0xffffffffu;
+    *hc = h;
+    if (cudaMemcpyAsync(ctl.p, hc, sizeof(PeelCtl), cudaMemcpyHostToDevice, st) != cudaSuccess) {
+      s = MCE_ERR_CUDA;
+      break;
+    }
+    k_peel_level<<<blocks, 256, 0, st>>>(k, remA.p, nrem, remB.p, off, adj, deg.p, state.p, order, ctl.p,
+                                          total_warps, spin_limit);
+    if (cudaGetLastError() != cudaSuccess) {
+      s = MCE_ERR_CUDA;
+      break;
+    }
+    if (cudaMemcpyAsync(hc, ctl.p, sizeof(PeelCtl), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+      s = MCE_ERR_CUDA;
+      break;
+    }
+    h = *hc;
+    if (h.error) {
+      s = MCE_ERR_TIMEOUT;
+      break;
+    }
+    tail = h.tail;
+    nrem = h.next_n;
+    std::swap(remA.p, remB.p);
+    if (h.claimed) {
+      degen = k;
+      k = k + 1;
+    } else {
+      if (h.min_rest == 0xffffffffu) break;
+      k = std::max(k + 1, h.min_rest);
+    }
+  }
+  cudaFreeHost(hc);
+  if (s == MCE_OK && tail != n) s = MCE_ERR_INTERNAL;
+  *degeneracy = degen;
+  return s;
+}
+
+}  // namespace
+
+mce_status build_from_pairs(const uint32_t *u, const uint32_t *v, uint64_t np, int order_kind,
+                            uint64_t spin_limit, cudaStream_t st, DeviceGraph *g) {
+  *g = DeviceGraph{};
+  DevBuf<uint32_t> maxbuf;
+  MCE_TRY(maxbuf.alloc(2, st));
+  MCE_TRY(reduce_max_u32(u, np, maxbuf.p, st));
+  MCE_TRY(reduce_max_u32(v, np, maxbuf.p + 1, st));
+  uint32_t hm[2] = {0, 0};
+  MCE_CUDA_TRY(cudaMemcpyAsync(hm, maxbuf.p, sizeof(hm), cudaMemcpyDeviceToHost, st));
+  MCE_CUDA_TRY(cudaStreamSynchronize(st));
+  const uint32_t maxlab = std::max(hm[0], hm[1]);
+  const int lb = bits_for(maxlab);
+  if (2 * lb > 63) return MCE_ERR_TOO_LARGE;
+
+  // 1) normalised (min,max) keys, sorted, unique
+  DevBuf<uint64_t> keys, tmp;
+  MCE_TRY(keys.alloc(np, st));
+  MCE_TRY(tmp.alloc(np, st));
+  k_pack_keys<<<grid_for(np, 256), 256, 0, st>>>(u, v, np, lb, keys.p);
+  MCE_TRY(radix_sort_u64(keys.p, tmp.p, np, 2 * lb, st));
+  DevBuf<uint32_t> flags, pos;
+  MCE_TRY(flags.alloc(np + 1, st));
+  MCE_TRY(pos.alloc(np + 1, st));
+  k_unique_flags<<<grid_for(np, 256), 256, 0, st>>>(keys.p, np, flags.p);
+  MCE_TRY(scan_exclusive_u32(flags.p, pos.p, np, pos.p + np, st));
+  uint32_t m32 = 0;
+  MCE_TRY(read_scalar(pos.p + np, &m32, st));
+  const uint64_t m = m32;
+  if (np > 0xffffffffULL || 2 * m >= (1ULL << 32)) return MCE_ERR_TOO_LARGE;
+  DevBuf<uint64_t> edges;
+  MCE_TRY(edges.alloc(m, st));
+  k_compact_keys<<<grid_for(np, 256), 256, 0, st>>>(keys.p, flags.p, pos.p, np, edges.p);
+  keys.release();
+  tmp.release();
+  flags.release();
+  pos.release();
+
+  // 2) dense ids of present labels, ascending (src/graph.cc:175-181)
+  const uint64_t nl = (uint64_t)maxlab + 1;
+  DevBuf<uint32_t> mark, id;
+  MCE_TRY(mark.alloc(nl + 1, st));
+  MCE_TRY(id.alloc(nl + 1, st));
+  MCE_CUDA_TRY(cudaMemsetAsync(mark.p, 0, nl * sizeof(uint32_t), st));
+  k_mark_labels<<<grid_for(m, 256), 256, 0, st>>>(edges.p, m, lb, mark.p);
+  MCE_TRY(scan_exclusive_u32(mark.p, id.p, nl, id.p + nl, st));
+  uint32_t n = 0;
+  MCE_TRY(read_scalar(id.p + nl, &n, st));
+  DevBuf<uint32_t> labels0, eu, ev, deg;
+  MCE_TRY(labels0.alloc(n, st));
+  MCE_TRY(eu.alloc(m, st));
+  MCE_TRY(ev.alloc(m, st));
+  MCE_TRY(deg.alloc(n + 1, st));
+  k_labels_from_marks<<<grid_for(nl, 256), 256, 0, st>>>(mark.p, id.p, nl, labels0.p);
+  MCE_CUDA_TRY(cudaMemsetAsync(deg.p, 0, (n + 1) * sizeof(uint32_t), st));
+  k_map_edges<<<grid_for(m, 256), 256, 0, st>>>(edges.p, m, lb, id.p, eu.p, ev.p, deg.p);
+  mark.release();
+  id.release();
+  edges.release();
+  MCE_TRY(finish_graph(n, m, eu.p, ev.p, deg.p, labels0.p, order_kind, spin_limit, st, g));
+  return MCE_OK;
+}
+
+// eu/ev: m edges on dense ids (any order, no duplicates, no self-loops);
+// deg: degrees (n); labels0: original labels of the dense ids.
+mce_status finish_graph(uint32_t n, uint64_t m, const uint32_t *eu, const uint32_t *ev, const uint32_t *deg,
+                        const uint32_t *labels0, int order_kind, uint64_t spin_limit, cudaStream_t st,
+                        DeviceGraph *g) {
+  *g = DeviceGraph{};
+  g->n = n;
+  g->m = m;
+  g->stream = st;
+  if (2 * m >= (1ULL << 32)) return MCE_ERR_TOO_LARGE;
+  DevBuf<uint32_t> maxd;
+  MCE_TRY(maxd.alloc(1, st));
+  MCE_TRY(reduce_max_u32(deg, n, maxd.p, st));
+  MCE_TRY(read_scalar(maxd.p, &g->max_degree, st));
+
+  // 3) vertex order
+  DevBuf<uint32_t> order, rank;
+  MCE_TRY(order.alloc(n, st));
+  MCE_TRY(rank.alloc(n, st));
+  g->degeneracy = g->max_degree;  // Graph::LoadFromFile leaves degeneracy_ = max degree (graph.cc:201)
+  if (order_kind == MCE_ORDER_DEGENERACY && n > 0) {
+    DevBuf<uint32_t> off0, cursor, adj0;
+    MCE_TRY(off0.alloc(n + 1, st));
+    MCE_TRY(cursor.alloc(n + 1, st));
+    MCE_TRY(adj0.alloc(2 * m, st));
+    MCE_TRY(scan_exclusive_u32(deg, off0.p, n, off0.p + n, st));
+    MCE_CUDA_TRY(cudaMemcpyAsync(cursor.p, off0.p, (n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    k_fill_adj<<<grid_for(m, 256), 256, 0, st>>>(eu, ev, m, cursor.p, adj0.p);
+    MCE_TRY(peel(n, off0.p, adj0.p, deg, order.p, &g->degeneracy, spin_limit, st));
+  } else if ((order_kind == MCE_ORDER_DEGREE_ASC || order_kind == MCE_ORDER_DEGREE_DESC) && n > 0) {
+    DevBuf<uint64_t> dk, dt;
+    MCE_TRY(dk.alloc(n, st));
+    MCE_TRY(dt.alloc(n, st));
+    k_degree_keys<<<grid_for(n, 256), 256, 0, st>>>(deg, n, order_kind == MCE_ORDER_DEGREE_DESC, dk.p);
+    MCE_TRY(radix_sort_u64(dk.p, dt.p, n, 64, st));
+    k_order_from_keys<<<grid_for(n, 256), 256, 0, st>>>(dk.p, n, order.p);
+  } else {
+    k_iota<<<grid_for(n, 256), 256, 0, st>>>(order.p, n);
+  }
+  k_rank_from_order<<<grid_for(n, 256), 256, 0, st>>>(order.p, n, rank.p);
+  order.release();
+
+  // 4) relabelled symmetric edge keys -> sorted CSR
+  const int nb = bits_for(n ? n - 1 : 0);
+  const uint64_t m2 = 2 * m;
+  DevBuf<uint64_t> keys, tmp;
+  MCE_TRY(keys.alloc(m2, st));
+  MCE_TRY(tmp.alloc(m2, st));
+  DevBuf<uint32_t> deg_new;
+  MCE_TRY(deg_new.alloc(n + 1, st));
+  MCE_CUDA_TRY(cudaMemsetAsync(deg_new.p, 0, (n + 1) * sizeof(uint32_t), st));
+  k_relabel_keys<<<grid_for(m, 256), 256, 0, st>>>(eu, ev, m, rank.p, nb, keys.p, deg_new.p);
+  MCE_TRY(radix_sort_u64(keys.p, tmp.p, m2, 2 * nb, st));
+  tmp.release();
+  MCE_CUDA_TRY(cudaMallocAsync(&g->off, (n + 1) * sizeof(uint32_t), st));
+  MCE_CUDA_TRY(cudaMallocAsync(&g->adj, std::max<uint64_t>(m2, 1) * sizeof(uint32_t), st));
+  MCE_TRY(scan_exclusive_u32(deg_new.p, g->off, n, g->off + n, st));
+  DevBuf<uint32_t> upflag, uppos;
+  MCE_TRY(upflag.alloc(m2 + 1, st));
+  MCE_TRY(uppos.alloc(m2 + 1, st));
+  k_csr_cols<<<grid_for(m2, 256), 256, 0, st>>>(keys.p, m2, nb, g->adj, upflag.p);
+  MCE_TRY(scan_exclusive_u32(upflag.p, uppos.p, m2, uppos.p + m2, st));
+  MCE_CUDA_TRY(cudaMallocAsync(&g->root_v0, std::max<uint64_t>(m, 1) * sizeof(uint32_t), st));
+  MCE_CUDA_TRY(cudaMallocAsync(&g->root_v1, std::max<uint64_t>(m, 1) * sizeof(uint32_t), st));
+  k_roots<<<grid_for(m2, 256), 256, 0, st>>>(keys.p, m2, nb, upflag.p, uppos.p, g->root_v0, g->root_v1);
+  keys.release();
+
+  // 5) labels and their hashes under the new ids
+  MCE_CUDA_TRY(cudaMallocAsync(&g->labels, std::max<uint32_t>(n, 1) * sizeof(uint32_t), st));
+  MCE_CUDA_TRY(cudaMallocAsync(&g->h1, std::max<uint32_t>(n, 1) * sizeof(uint64_t), st));
+  MCE_CUDA_TRY(cudaMallocAsync(&g->h2, std::max<uint32_t>(n, 1) * sizeof(uint64_t), st));
+  k_permute_labels<<<grid_for(n, 256), 256, 0, st>>>(labels0, rank.p, n, g->labels, g->h1, g->h2);
+  MCE_CUDA_TRY(cudaGetLastError());
+  MCE_CUDA_TRY(cudaStreamSynchronize(st));
+  return MCE_OK;
+}
+
+// CSR given by the caller (rows sorted).  already_ordered: use ids as given.
+mce_status build_from_csr(uint64_t n, const uint32_t *off_d, const uint32_t *adj_d, const uint32_t *labels_d,
+                          int already_ordered, int order_kind, uint32_t degeneracy_hint, uint64_t spin_limit,
+                          cudaStream_t st, DeviceGraph *g) {
+  *g = DeviceGraph{};
+  uint32_t m2 = 0;
+  MCE_CUDA_TRY(cudaMemcpyAsync(&m2, off_d + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  MCE_CUDA_TRY(cudaStreamSynchronize(st));
+  const uint64_t m = m2 / 2;
+  // edges (r < c) and degrees from the CSR
+  DevBuf<uint32_t> deg, eu, ev, labels0;
+  MCE_TRY(deg.alloc(n + 1, st));
+  MCE_TRY(labels0.alloc(n, st));
+  if (labels_d)
+    MCE_CUDA_TRY(cudaMemcpyAsync(labels0.p, labels_d, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+  else
+    k_iota<<<grid_for(n, 256), 256, 0, st>>>(labels0.p, n);
+  MCE_TRY(csr_to_edges(n, off_d, adj_d, m, deg.p, &eu.p, &ev.p, st));
+  eu.st = ev.st = st;
+  MCE_TRY(finish_graph((uint32_t)n, m, eu.p, ev.p, deg.p, labels0.p,
+                       already_ordered ? MCE_ORDER_UNCHANGED : order_kind, spin_limit, st, g));
+  if (already_ordered && degeneracy_hint) g->degeneracy = degeneracy_hint;
+  return MCE_OK;
+}
+
+namespace {
+__global__ void k_degrees_from_off(const uint32_t *off, uint64_t n, uint32_t *deg) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    deg[i] = off[i + 1] - off[i];
+}
+__global__ void k_upper_flags(const uint32_t *off, const uint32_t *adj, uint64_t n, uint32_t *flag) {
+  // one warp per row
+  const uint32_t lane = lane_id();
+  for (uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n;
+       r += ((uint64_t)gridDim.x * blockDim.x) >> 5)
+    for (uint32_t e = off[r] + lane; e < off[r + 1]; e += 32) flag[e] = adj[e] > r ? 1u : 0u;
+}
+__global__ void k_upper_edges(const uint32_t *off, const uint32_t *adj, uint64_t n, const uint32_t *flag,
+                              const uint32_t *pos, uint32_t *eu, uint32_t *ev) {
+  const uint32_t lane = lane_id();
+  for (uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n;
+       r += ((uint64_t)gridDim.x * blockDim.x) >> 5)
+    for (uint32_t e = off[r] + lane; e < off[r + 1]; e += 32)
+      if (flag[e]) {
+        eu[pos[e]] = (uint32_t)r;
+        ev[pos[e]] = adj[e];
+      }
+}
+}  // namespace
+
+mce_status csr_to_edges(uint64_t n, const uint32_t *off, const uint32_t *adj, uint64_t m, uint32_t *deg,
+                        uint32_t **eu, uint32_t **ev, cudaStream_t st) {
+  k_degrees_from_off<<<grid_for(n, 256), 256, 0, st>>>(off, n, deg);
+  DevBuf<uint32_t> flag, pos;
+  MCE_TRY(flag.alloc(2 * m + 1, st));
+  MCE_TRY(pos.alloc(2 * m + 1, st));
+  k_upper_flags<<<grid_for(n * 32, 256), 256, 0, st>>>(off, adj, n, flag.p);
+  MCE_TRY(scan_exclusive_u32(flag.p, pos.p, 2 * m, pos.p + 2 * m, st));
+  uint32_t mu = 0;
+  MCE_TRY(read_scalar(pos.p + 2 * m, &mu, st));
+  if (mu != m) return MCE_ERR_FORMAT;  // not symmetric / has self-loops
+  MCE_CUDA_TRY(cudaMallocAsync(eu, std::max<uint64_t>(m, 1) * sizeof(uint32_t), st));
+  MCE_CUDA_TRY(cudaMallocAsync(ev, std::max<uint64_t>(m, 1) * sizeof(uint32_t), st));
+  k_upper_edges<<<grid_for(n * 32, 256), 256, 0, st>>>(off, adj, n, flag.p, pos.p, *eu, *ev);
+  MCE_CUDA_TRY(cudaGetLastError());
+  return MCE_OK;
+}
+
+void free_graph(DeviceGraph *g) {
+  cudaStream_t st = g->stream;
+  cudaFreeAsync(g->off, st);
+  cudaFreeAsync(g->adj, st);
+  cudaFreeAsync(g->labels, st);
+  cudaFreeAsync(g->h1, st);
+  cudaFreeAsync(g->h2, st);
+  cudaFreeAsync(g->root_v0, st);
+  cudaFreeAsync(g->root_v1, st);
+  if (g->slot) cudaFreeAsync(g->slot, st);
+  *g = DeviceGraph{};
+}
+
+}  // namespace mce
