@@ -11,10 +11,18 @@
 //                                    root-parallel: one MceSolver per thread, the
 //                                    vertex roots of src/mce.cc:66-95 handed out in
 //                                    chunks, each solved by BKFixedMemPivotBit2
+//   ref_cpu steps <graph> <threads> <seconds> <warmup> <steps>
+//                                    bench steps: each step (a forked child)
+//                                    solves vertex roots in a seeded random order
+//                                    with all threads until <seconds>, then
+//                                    reports the cliques found so far and exits
 //   ref_cpu stats <graph>            n, m, max degree, degeneracy after the sort
 //   ref_cpu csr <graph> <out>        CSR + labels after the sort (binary dump)
 // <graph> is COO text (sorted by degeneracy as main.cc:26-27 does) or a .bin.
 #include <atomic>
+#include <random>
+#include <sys/wait.h>
+#include <unistd.h>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -135,6 +143,66 @@ int main(int argc, char **argv) {
     for (auto c : counts) total += c;
     std::printf("RESULT count %llu seconds %.6f threads %d roots %llu\n", (unsigned long long)total, sec,
                 threads, (unsigned long long)limit);
+    return 0;
+  }
+  if (mode == "steps") {
+    if (argc < 7) return 2;
+    const int threads = std::max(1, std::atoi(argv[3]));
+    const double seconds = std::atof(argv[4]);
+    const int total_steps = std::atoi(argv[5]) + std::atoi(argv[6]);
+    const uint64_t n = g.GetNumVertices();
+    std::vector<vid_t> order(n);
+    for (uint64_t i = 0; i < n; i++) order[i] = (vid_t)i;
+    std::mt19937_64 rng(12345);
+    std::shuffle(order.begin(), order.end(), rng);
+    for (int step = 0; step < total_steps; step++) {
+      std::fflush(stdout);
+      pid_t pid = fork();
+      if (pid < 0) return 1;
+      if (pid == 0) {
+        // a single vertex root can take hours: threads are detached and the
+        // child reports the cliques counted so far at the deadline, then exits
+        std::atomic<uint64_t> next(0);
+        std::vector<std::unique_ptr<MceSolver>> solvers;
+        for (int t = 0; t < threads; t++) solvers.emplace_back(new MceSolver(g));
+        auto t0 = std::chrono::steady_clock::now();
+        for (int t = 0; t < threads; t++) {
+          std::thread([&, t]() {
+            MceSolver &s = *solvers[t];
+            for (;;) {
+              uint64_t k = next.fetch_add(1);
+              if (k >= n) break;
+              vid_t v0 = order[k];
+              vlist_t R, P, X;
+              R.emplace_back(v0);
+              for (vid_t v1 : g.N(v0)) {
+                if (v0 > v1) X.emplace_back(v1);
+                else P.emplace_back(v1);
+              }
+              if (P.empty()) {
+                if (X.empty()) s.IncrementMceCount();
+                continue;
+              }
+              s.BKFixedMemPivotBit2(R, P, X);
+            }
+          }).detach();
+        }
+        for (;;) {
+          std::this_thread::sleep_for(std::chrono::milliseconds(50));
+          double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+          if (el >= seconds || next.load() >= n + (uint64_t)threads) {
+            uint64_t total = 0;
+            for (auto &sv : solvers) total += *(volatile acc_t *)&sv->mce_count_;
+            std::printf("STEP %d cliques %llu seconds %.6f roots %llu\n", step, (unsigned long long)total, el,
+                        (unsigned long long)std::min<uint64_t>(next.load(), n));
+            std::fflush(stdout);
+            _exit(0);
+          }
+        }
+      }
+      int status = 0;
+      waitpid(pid, &status, 0);
+    }
     return 0;
   }
   std::fprintf(stderr, "unknown mode %s\n", mode.c_str());
