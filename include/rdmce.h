@@ -92,6 +92,11 @@ typedef struct mce_result {
   uint64_t roots;             /* roots enumerated */
   uint64_t shared_tasks;      /* tasks handed between warps */
   uint64_t heavy_roots;       /* roots that went through the large-scratch pass */
+  uint64_t nodes;             /* search-tree nodes visited */
+  uint64_t word_ops;          /* 64-bit bitmap word operations (AND/ANDN/POPC on rows) */
+  uint64_t launches;          /* enumeration kernel launches */
+  uint64_t warp_cycles[6];    /* warp clock cycles by phase: root build, register tiers,
+                                 general tier, exposing tasks, idle, queue */
   double phase_ms[MCE_PHASES];
   uint64_t hist[MCE_HIST_LEN];
 } mce_result;
@@ -110,6 +115,11 @@ void mce_default_options(mce_options *opt);
 const char *mce_status_str(mce_status s);
 /* Library version string. */
 const char *mce_version(void);
+/* Kernels the engine has launched in this process (for launch accounting). */
+uint64_t mce_launch_count(void);
+/* Measured throughput of the enumeration's word-op mix (64-bit ANDN + POPC),
+ * in word-ops per second: the integer-pipe roof of the enumeration kernel. */
+mce_status mce_probe_int_peak(int device, double *word_ops_per_s);
 
 /* COO pairs in host memory -> device-resident, degeneracy-ordered CSR.
  * Replaces Graph::LoadFromFile's edge handling + SortByOrder + ConvertToCsr +
@@ -155,6 +165,11 @@ mce_status mce_solve(mce_graph *g, const mce_options *opt, mce_result *out);
  * undirected edge v0 < v1, numbered in CSR order).  For sampled-root parity. */
 mce_status mce_solve_roots(mce_graph *g, const uint64_t *roots, uint64_t n_roots, const mce_options *opt,
                            uint64_t *counts, uint64_t *checksums);
+
+/* Enumerate the maximal cliques rooted at an explicit set of roots (sampled
+ * solves).  Totals only; root ids as in mce_solve_roots. */
+mce_status mce_solve_root_list(mce_graph *g, const uint64_t *roots, uint64_t n_roots, const mce_options *opt,
+                               mce_result *out);
 
 /* One call: host COO -> result, everything on the device in between. */
 mce_status mce_solve_coo(const uint32_t *u, const uint32_t *v, uint64_t n_pairs, const mce_options *opt,

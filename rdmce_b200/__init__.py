@@ -69,6 +69,10 @@ class _Result(C.Structure):
         ("roots", C.c_uint64),
         ("shared_tasks", C.c_uint64),
         ("heavy_roots", C.c_uint64),
+        ("nodes", C.c_uint64),
+        ("word_ops", C.c_uint64),
+        ("launches", C.c_uint64),
+        ("warp_cycles", C.c_uint64 * 6),
         ("phase_ms", C.c_double * PHASES),
         ("hist", C.c_uint64 * HIST_LEN),
     ]
@@ -117,12 +121,18 @@ class Result:
     shared_tasks: int = 0
     heavy_roots: int = 0
     phase_ms: list = field(default_factory=list)
+    nodes: int = 0
+    word_ops: int = 0
+    launches: int = 0
+    # warp clock cycles: root build, register tiers, general tier, exposing tasks, idle, queue
+    warp_cycles: list = field(default_factory=list)
 
     @classmethod
     def _from(cls, r: _Result) -> "Result":
         hist = {s: int(r.hist[s]) for s in range(HIST_LEN) if r.hist[s]}
         return cls(r.count, r.checksum, hist, r.max_size, r.degeneracy, r.max_degree, r.num_vertices,
-                   r.num_edges, r.roots, r.shared_tasks, r.heavy_roots, list(r.phase_ms))
+                   r.num_edges, r.roots, r.shared_tasks, r.heavy_roots, list(r.phase_ms), r.nodes, r.word_ops,
+                   r.launches, list(r.warp_cycles))
 
 
 _lib = None
@@ -143,6 +153,9 @@ _SIGS = {
     "mce_graph_free": (None, [_P]),
     "mce_solve": (_I, [_P, C.POINTER(Options), C.POINTER(_Result)]),
     "mce_solve_roots": (_I, [_P, _P, _U64, C.POINTER(Options), _P, _P]),
+    "mce_solve_root_list": (_I, [_P, _P, _U64, C.POINTER(Options), C.POINTER(_Result)]),
+    "mce_launch_count": (_U64, []),
+    "mce_probe_int_peak": (_I, [_I, C.POINTER(_D)]),
     "mce_solve_coo": (_I, [_P, _P, _U64, C.POINTER(Options), C.POINTER(_Result)]),
     "mce_batch_create": (_I, [_P, _P, _P, _U32, C.POINTER(Options), C.POINTER(_P)]),
     "mce_batch_solve": (_I, [_P, C.POINTER(Options), _P, _P, _U32, C.POINTER(_D)]),
@@ -367,6 +380,26 @@ class Graph:
         _check(lib().mce_solve_roots(self.h, _ptr(roots), len(roots), C.byref(opts) if opts else None, _ptr(cnt),
                                      _ptr(chk)), "mce_solve_roots")
         return cnt, chk
+
+    def solve_root_list(self, roots, opts: Options | None = None) -> Result:
+        """Enumerate only the listed roots (indices into the degeneracy-ordered edge list)."""
+        roots = np.ascontiguousarray(roots, dtype=np.uint64)
+        r = _Result()
+        _check(lib().mce_solve_root_list(self.h, _ptr(roots), len(roots), C.byref(opts) if opts else None,
+                                         C.byref(r)), "mce_solve_root_list")
+        return Result._from(r)
+
+
+def launch_count() -> int:
+    """Kernels this process has launched through the engine so far."""
+    return int(lib().mce_launch_count())
+
+
+def probe_int_peak(device: int = 0) -> float:
+    """Measured 64-bit ANDN+POPC word-op throughput of the device (ops/s)."""
+    d = C.c_double()
+    _check(lib().mce_probe_int_peak(device, C.byref(d)), "mce_probe_int_peak")
+    return d.value
 
 
 def solve_coo(u, v, opts: Options | None = None) -> Result:

@@ -107,6 +107,12 @@ extern "C" {
 
 const char *mce_version(void) { return "rdmce_b200 0.1 (sm_100a)"; }
 
+mce_status mce_probe_int_peak(int device, double *word_ops_per_s) {
+  if (!word_ops_per_s) return MCE_ERR_INVALID_ARG;
+  MCE_TRY(set_device(device));
+  return probe_int_peak(device, word_ops_per_s);
+}
+
 void mce_default_options(mce_options *opt) {
   if (opt) *opt = defaults();
 }
@@ -339,6 +345,10 @@ static mce_status solve_impl(mce_graph *g, const mce_options &o, mce_result *out
   out->roots = stats.roots;
   out->heavy_roots = stats.heavy_roots;
   out->shared_tasks = stats.shared_tasks;
+  out->nodes = stats.nodes;
+  out->word_ops = stats.word_ops;
+  out->launches = stats.launches;
+  for (int i = 0; i < 6; i++) out->warp_cycles[i] = stats.cycles[i];
   out->status_detail = stats.error;
   out->phase_ms[MCE_PHASE_H2D] = g->ms_h2d;
   out->phase_ms[MCE_PHASE_PREPROCESS] = g->ms_pre;
@@ -391,6 +401,26 @@ mce_status mce_solve_roots(mce_graph *g, const uint64_t *roots, uint64_t n_roots
   if (rd) cudaFreeAsync(rd, st);
   if (cd) cudaFreeAsync(cd, st);
   if (hd) cudaFreeAsync(hd, st);
+  cudaStreamSynchronize(st);
+  return s;
+}
+
+mce_status mce_solve_root_list(mce_graph *g, const uint64_t *roots, uint64_t n_roots, const mce_options *opt,
+                               mce_result *out) {
+  if (!g || !out || (n_roots && !roots)) return MCE_ERR_INVALID_ARG;
+  for (uint64_t i = 0; i < n_roots; i++)
+    if (roots[i] >= g->g.m) return MCE_ERR_INVALID_ARG;
+  mce_options tmp;
+  const mce_options &o = opts_or_default(opt, tmp);
+  MCE_CUDA_TRY(cudaSetDevice(g->device));
+  cudaStream_t st = g->stream;
+  uint64_t *rd = nullptr;
+  if (cudaMallocAsync(&rd, std::max<uint64_t>(n_roots, 1) * 8, st) != cudaSuccess) return MCE_ERR_OUT_OF_MEMORY;
+  mce_status s = MCE_OK;
+  if (n_roots && cudaMemcpyAsync(rd, roots, n_roots * 8, cudaMemcpyHostToDevice, st) != cudaSuccess)
+    s = MCE_ERR_CUDA;
+  if (s == MCE_OK) s = solve_impl(g, o, out, rd, n_roots, nullptr, nullptr);
+  cudaFreeAsync(rd, st);
   cudaStreamSynchronize(st);
   return s;
 }

@@ -144,8 +144,8 @@ mce_status mce_batch_create(const uint32_t *u, const uint32_t *v, const uint64_t
     s = MCE_ERR_CUDA;
   if (s == MCE_OK) {
     const uint32_t gb = std::min<uint32_t>(n_graphs, 148 * 32);
-    k_graph_max_label<<<gb, 256, 0, st>>>(ud, vd, pd, n_graphs, gmax);
-    k_plus_one<<<grid_for(n_graphs, 256), 256, 0, st>>>(gmax, n_graphs, pd);
+    k_graph_max_label<<<gb, 256, 0, st>>>(ud, vd, pd, n_graphs, gmax); note_launch();
+    k_plus_one<<<grid_for(n_graphs, 256), 256, 0, st>>>(gmax, n_graphs, pd); note_launch();
     // label_base = exclusive prefix of (max label + 1); the total must fit in 32 bits
     s = scan_exclusive_u32(gmax, b->label_base, n_graphs, b->label_base + n_graphs, st);
   }
@@ -161,7 +161,7 @@ mce_status mce_batch_create(const uint32_t *u, const uint32_t *v, const uint64_t
   }
   if (s == MCE_OK) {
     const uint32_t gb = std::min<uint32_t>(n_graphs, 148 * 32);
-    k_shift_pairs<<<gb, 256, 0, st>>>(ud, vd, pd, n_graphs, b->label_base);
+    k_shift_pairs<<<gb, 256, 0, st>>>(ud, vd, pd, n_graphs, b->label_base); note_launch();
     s = build_from_pairs(ud, vd, np, o.order, o.spin_limit ? o.spin_limit : (1ULL << 34), st, &b->g);
   }
   cudaFreeAsync(ud, st);
@@ -182,9 +182,9 @@ mce_status mce_batch_create(const uint32_t *u, const uint32_t *v, const uint64_t
   cudaMemsetAsync(nvd, 0, n_graphs * 4ULL, st);
   cudaMemsetAsync(ned, 0, n_graphs * 8ULL, st);
   k_local_labels<<<grid_for(b->g.n, 256), 256, 0, st>>>(b->g.labels, b->g.h1, b->g.h2, b->g.slot, b->g.n,
-                                                          b->label_base, n_graphs);
+                                                          b->label_base, n_graphs); note_launch();
   k_count_per_graph<<<grid_for(std::max<uint64_t>(b->g.n, b->g.m), 256), 256, 0, st>>>(b->g.slot, b->g.n,
-                                                                                      b->g.root_v0, b->g.m, nvd, ned);
+                                                                                      b->g.root_v0, b->g.m, nvd, ned); note_launch();
   b->nv.resize(n_graphs);
   b->ne.resize(n_graphs);
   if (cudaMemcpyAsync(b->nv.data(), nvd, n_graphs * 4ULL, cudaMemcpyDeviceToHost, st) != cudaSuccess ||

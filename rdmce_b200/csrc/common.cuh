@@ -127,6 +127,9 @@ Scratch *default_scratch(int device);
 void lock_default(int device);
 void unlock_default(int device);
 
+// every kernel launch of the engine is counted (mce_launch_count)
+void note_launch();
+
 inline uint32_t grid_for(uint64_t n, uint32_t block, uint32_t cap = 148u * 64u) {
   uint64_t g = (n + block - 1) / block;
   if (g < 1) g = 1;

@@ -60,6 +60,8 @@ struct EnumStats {
   uint64_t roots = 0;
   uint64_t heavy_roots = 0;
   uint64_t shared_tasks = 0;
+  uint64_t nodes = 0, word_ops = 0;
+  uint64_t cycles[6] = {0, 0, 0, 0, 0, 0};
   uint32_t error = 0;
   float ms_setup = 0, ms_enum = 0;
   uint64_t launches = 0;
@@ -95,8 +97,24 @@ struct EnumParams {
   unsigned long long *per_root_count;
   unsigned long long *per_root_checksum;
   int expand_r;
+  int sharing;                           // root-down exposure through the task pool
+  uint32_t share_bound;                  // expose only levels with |P| >= this
+  uint32_t nwarps;
+  uint64_t spin_limit;                   // bound on every device-side wait
   unsigned int *error;
   unsigned long long *stat_roots;
+  unsigned long long *stat_tasks;
+  unsigned long long *stat_nodes;
+  unsigned long long *stat_wops;
+  unsigned long long *stat_cycles;       // per phase: build, register tiers, general tier, spawn, idle, queue
+  unsigned int *active;                  // warps holding work
+  // task pool: blocks of block_bytes, a free ring and a ready ring (one cell per block)
+  char *pool;
+  uint32_t block_bytes;
+  uint32_t pool_mask;
+  uint32_t *free_slot, *ready_slot;
+  unsigned long long *free_seq, *ready_seq;
+  unsigned long long *free_head, *free_tail, *ready_head, *ready_tail;
 };
 
 
@@ -109,6 +127,7 @@ struct EnumPlan {
   size_t smem = 0;
   uint64_t nwarps = 0, nwork = 0;
   bool fits_all = false;  // every root fits the normal slab: no deferred pass possible
+  uint32_t pool_blocks = 0;
   void *ctl = nullptr;
   Scratch *scr = nullptr;
 };
@@ -121,5 +140,6 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
                      unsigned long long *hist, EnumPlan *plan);
 mce_status enum_launch(const EnumPlan &plan, cudaStream_t st);
 mce_status enum_finish(const EnumPlan &plan, cudaStream_t st, EnumStats *stats);
+mce_status probe_int_peak(int device, double *word_ops_per_s);
 
 }  // namespace mce

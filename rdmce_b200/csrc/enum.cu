@@ -9,20 +9,32 @@
 //   node: pivot = argmin over rows containing R of |P \ row| (:229-257),
 //   branch on VP = P \ row(pivot) in ascending order; child P' = P & row(q);
 //   EXPAND_R moves every i in P' with |P' \ row(i)| == 1 into R (:368-382);
-//   leaf: P empty and no row contains R -> one maximal clique (:276-294).
+//   leaf: P empty and no row contains R -> one maximal clique (:276-294);
+//   root-down exposure: the shallowest level with open candidates is handed
+//   to other warps when they run dry (:87-138, :552-598).
 //
-// B200 design differences:
-//   * each level keeps the list of rows that contain R ("active rows"), so a
-//     pivot scan reads only candidate rows instead of every row with an
-//     R-subset test; if the per-warp list space runs out a level inherits its
-//     parent's list and falls back to the subset test (never a skipped root);
-//   * ties in the pivot go to the lowest row index (canonical, matches the
-//     CPU oracle's node counts);
-//   * every leaf also feeds a clique-size histogram and the order-independent
-//     checksum (mix64 set hash over original labels);
-//   * scratch is sized per root: roots whose ego network exceeds the per-warp
-//     slab are deferred to a second pass with large slabs, never skipped
-//     (the reference prints and skips them, :480-487).
+// B200 design:
+//   * Three tiers by subproblem size.  Nearly every search-tree node has at
+//     most 32 candidate columns and 32 rows that contain R: there each lane
+//     holds one row as a 32-bit word, P / VP / the active-row set are
+//     warp-uniform 32-bit masks, and a node is one redux.sync (pivot argmin),
+//     one ballot (the child's active rows) and a few shuffles.  Up to 64
+//     columns and 128 rows, each lane holds 4 rows as 64-bit words.  Larger
+//     subproblems run in the general tier (W 64-bit words per row in a global
+//     scratch slab, per-level lists of active rows).  A child small enough for
+//     a smaller tier has its rows compressed to its own columns (parallel bit
+//     compress) and gathered, and continues there.
+//   * Root-down exposure with self-contained tasks.  When warps are idle, a
+//     busy warp turns every open candidate of its shallowest level with
+//     |P| >= tau into a task record (rows restricted to the child's columns)
+//     in a global pool, published through lock-free bounded MPMC rings.  A
+//     task owns its data, so no warp ever waits on another warp's stack (the
+//     reference's owner waits for its thieves, :87-138).  Every wait is bounded.
+//   * Pivot ties go to the lowest row index; every leaf feeds the clique-size
+//     histogram and the order-independent checksum.
+//   * Roots whose ego network exceeds the per-warp slab are deferred to a
+//     second pass with large slabs, never skipped (the reference prints and
+//     skips them, :480-487).
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -32,97 +44,946 @@
 
 namespace mce {
 
-constexpr uint32_t kIdent = 0xffffffffu;  // level-0 list = all rows
-constexpr uint32_t kHistCache = 128;      // per-warp shared-memory histogram bins
-
 namespace {
 
-struct WarpAcc {
-  // lane-0 accumulators for the current result slot
-  unsigned long long count, checksum;
-  uint32_t max_size, slot, pending;
+constexpr uint32_t kIdent = 0xffffffffu;  // level-0 list = all rows
+constexpr uint32_t kHistCache = 128;      // per-warp shared-memory histogram bins
+constexpr int kRPL = 4;                   // 64-bit tier: rows per lane
+constexpr uint32_t kT1Rows = 32 * kRPL;   // 64-bit tier: rows per subproblem
+constexpr uint32_t kT1Depth = 66;         // 64-bit tier: levels (<= 64 columns + root)
+constexpr uint32_t kT0Depth = 34;         // 32-bit tier: levels (<= 32 columns + root)
+constexpr uint32_t kHdr = 64;             // task record header bytes
+constexpr uint32_t kLocalRec = 2048;      // per-warp local task record (64-bit-tier size)
+// phases of the per-warp cycle accounting
+enum { kCycBuild = 0, kCycReg = 1, kCycGen = 2, kCycSpawn = 3, kCycIdle = 4, kCycQueue = 5, kCycPhases = 6 };
+
+struct TaskHdr {
+  uint32_t pc;     // candidate columns
+  uint32_t nrows;  // rows: pc candidate rows, then the X rows
+  uint32_t W;      // 64-bit words per row
+  uint32_t rsize;  // |R| beyond the root edge
+  uint64_t s1, s2; // label-hash sums of the clique so far (root edge included)
+  uint32_t slot;   // result slot
+  uint32_t pad0;
+  uint64_t pad[3];
 };
-
-__device__ __forceinline__ void acc_flush(const EnumParams &P, WarpAcc &a, uint32_t *hcache, uint32_t lane) {
-  // all lanes: flush histogram cache; lane 0: flush scalars
-  __syncwarp();
-  for (uint32_t b = lane; b < kHistCache; b += 32) {
-    uint32_t c = hcache[b];
-    if (c) {
-      uint32_t bin = b < P.hist_len ? b : P.hist_len - 1;
-      atomicAdd(&P.hist[(uint64_t)a.slot * P.hist_len + bin], (unsigned long long)c);
-      hcache[b] = 0;
-    }
-  }
-  if (lane == 0 && (a.count || a.max_size)) {
-    atomicAdd(&P.slots[a.slot].count, a.count);
-    atomicAdd(&P.slots[a.slot].checksum, a.checksum);
-    atomicMax(&P.slots[a.slot].max_size, a.max_size);
-  }
-  a.count = 0;
-  a.checksum = 0;
-  a.max_size = 0;
-  a.pending = 0;
-  __syncwarp();
-}
-
-// lane 0 only
-__device__ __forceinline__ void emit(const EnumParams &P, WarpAcc &a, uint32_t *hcache, uint32_t size, uint64_t s1,
-                                     uint64_t s2) {
-  a.count++;
-  a.checksum += clique_hash(s1, s2, size);
-  a.max_size = max(a.max_size, size);
-  if (size < kHistCache) {
-    hcache[size]++;
-    a.pending++;
-  } else {
-    uint32_t bin = size < P.hist_len ? size : P.hist_len - 1;
-    atomicAdd(&P.hist[(uint64_t)a.slot * P.hist_len + bin], 1ULL);
-  }
-}
+static_assert(sizeof(TaskHdr) == kHdr, "task header is 64 bytes");
 
 __host__ __device__ __forceinline__ uint64_t align8(uint64_t x) { return (x + 7) & ~7ULL; }
 
-// Layout of one root inside a warp slab (bytes).
-struct RootLayout {
-  uint64_t hash_off, rows_off, stack_off, alist_off, alist_cap, need;
-};
-
-__device__ __forceinline__ RootLayout layout_for(uint64_t cand_n, uint32_t p, uint32_t x, uint32_t W) {
-  RootLayout L;
-  L.hash_off = align8(cand_n * 4);
-  L.rows_off = L.hash_off + 16ULL * p;
-  L.stack_off = L.rows_off + 8ULL * (uint64_t)(p + x) * W;
-  L.alist_off = L.stack_off + 8ULL * (uint64_t)(p + 2) * (3ULL * W + 4);
-  L.need = L.alist_off + 4ULL * (p + x);  // at least one full-size child list
-  L.alist_cap = 0;
-  return L;
+__host__ __device__ __forceinline__ uint64_t task_bytes(uint32_t pc, uint32_t nrows, uint32_t W) {
+  return kHdr + align8(4ULL * pc) + 8ULL * nrows * W;
 }
 
-// Solve one ego network already built in the slab.  All lanes participate.
-__device__ void solve_ego(const EnumParams &P, WarpAcc &acc, uint32_t *hcache, const uint64_t *rows,
-                          const uint64_t *h1s, const uint64_t *h2s, uint64_t *stack, uint32_t *alist,
-                          uint64_t alist_cap, uint32_t p, uint32_t nrows, uint32_t W, uint64_t s1_root,
-                          uint64_t s2_root) {
-  const uint32_t lane = lane_id();
-  const uint64_t LREC = 3ULL * W + 4;
-  // level 0: P = all p bits, R = 0, active rows = all rows
+// Per-warp shared memory.  All mutable per-warp state outside the tier loops
+// lives here (lane 0 updates the scalars), so the small Ctx handle can be
+// passed by value.
+struct WarpSmem {
+  uint64_t rowbuf[64];
+  // 64-bit tier frames
+  uint64_t fP[kT1Depth], fVP[kT1Depth], fs1[kT1Depth], fs2[kT1Depth];
+  uint32_t frs[kT1Depth];
+  uint8_t fab[kT1Depth][32];
+  // 32-bit tier frames: (P, VP, active rows, |R|) and (s1, s2)
+  uint4 t0f[kT0Depth];
+  ulonglong2 t0s[kT0Depth];
+  // exchange buffer for moving a subproblem into the 32-bit tier
+  uint32_t xrow[32], xcv[32];
+  uint64_t xh1[32], xh2[32];
+  uint32_t hcache[kHistCache];
+  // result accumulators for the current slot
+  unsigned long long count, checksum, nodes, wops;
+  uint32_t max_size, slot, pending, pad;
+  unsigned long long cyc[kCycPhases];  // clock64 cycles by phase
+};
+
+struct Ctx {
+  const EnumParams *P;
+  WarpSmem *sm;
+  char *slab;
+  uint64_t slab_bytes;
+  uint32_t lane;
+  bool sharing;
+};
+
+__device__ __forceinline__ unsigned long long now() { return clock64(); }
+
+// Task records travel between SMs through reused pool blocks; read them from
+// L2 (ld.global.cg) so no SM sees a stale L1 line of an earlier task.
+__device__ __forceinline__ uint64_t ld_cg(const uint64_t *p) { return __ldcg((const unsigned long long *)p); }
+__device__ __forceinline__ uint32_t ld_cg(const uint32_t *p) { return __ldcg((const unsigned int *)p); }
+
+// ------------------------------------------------------------ accounting
+
+__device__ __forceinline__ void acc_flush(const Ctx &c) {
+  const EnumParams &P = *c.P;
+  WarpSmem *sm = c.sm;
+  __syncwarp();
+  for (uint32_t b = c.lane; b < kHistCache; b += 32) {
+    const uint32_t n = sm->hcache[b];
+    if (n) {
+      const uint32_t bin = b < P.hist_len ? b : P.hist_len - 1;
+      atomicAdd(&P.hist[(uint64_t)sm->slot * P.hist_len + bin], (unsigned long long)n);
+      sm->hcache[b] = 0;
+    }
+  }
+  if (c.lane == 0) {
+    if (sm->count || sm->max_size) {
+      atomicAdd(&P.slots[sm->slot].count, sm->count);
+      atomicAdd(&P.slots[sm->slot].checksum, sm->checksum);
+      atomicMax(&P.slots[sm->slot].max_size, sm->max_size);
+    }
+    sm->count = 0;
+    sm->checksum = 0;
+    sm->max_size = 0;
+    sm->pending = 0;
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void set_slot(const Ctx &c, uint32_t slot) {
+  if (c.sm->slot != slot) {
+    acc_flush(c);
+    if (c.lane == 0) c.sm->slot = slot;
+    __syncwarp();
+  }
+}
+
+// lane 0 only
+__device__ __forceinline__ void emit(const Ctx &c, uint32_t size, uint64_t s1, uint64_t s2) {
+  WarpSmem *sm = c.sm;
+  sm->count++;
+  sm->checksum += clique_hash(s1, s2, size);
+  sm->max_size = max(sm->max_size, size);
+  if (size < kHistCache) {
+    sm->hcache[size]++;
+    sm->pending++;
+  } else {
+    const EnumParams &P = *c.P;
+    const uint32_t bin = size < P.hist_len ? size : P.hist_len - 1;
+    atomicAdd(&P.hist[(uint64_t)sm->slot * P.hist_len + bin], 1ULL);
+  }
+}
+
+__device__ __forceinline__ void maybe_flush(const Ctx &c) {
+  // keeps every u32 histogram bin far from overflow
+  if (c.sm->pending > (1u << 30)) acc_flush(c);
+}
+
+// ------------------------------------------------------- bounded MPMC rings
+// Vyukov's bounded queue: cell seq == pos means free for the producer of pos,
+// seq == pos + 1 means filled for the consumer of pos.  Lane 0 only.
+
+__device__ bool ring_push(uint32_t *slots, unsigned long long *seq, unsigned long long *tail, uint32_t mask,
+                          uint32_t val, const EnumParams &P) {
+  const unsigned long long pos = atomicAdd(tail, 1ULL);
+  volatile unsigned long long *s = seq + (pos & mask);
+  uint64_t n = 0;
+  while (*s != pos) {
+    if (++n > P.spin_limit) {
+      atomicExch(P.error, 3u);
+      return false;
+    }
+    __nanosleep(64);
+  }
+  ((volatile uint32_t *)slots)[pos & mask] = val;
+  __threadfence();
+  *s = pos + 1;
+  return true;
+}
+
+__device__ bool ring_pop(uint32_t *slots, unsigned long long *seq, unsigned long long *head,
+                         unsigned long long *tail, uint32_t mask, uint32_t *val, const EnumParams &P) {
+  for (int tries = 0; tries < 32; tries++) {
+    const unsigned long long h = *(volatile unsigned long long *)head;
+    const unsigned long long t = *(volatile unsigned long long *)tail;
+    if (h >= t) return false;
+    if (atomicCAS(head, h, h + 1) == h) {
+      volatile unsigned long long *s = seq + (h & mask);
+      uint64_t n = 0;
+      while (*s != h + 1) {
+        if (++n > P.spin_limit) {
+          atomicExch(P.error, 3u);
+          return false;
+        }
+        __nanosleep(32);
+      }
+      __threadfence();
+      *val = ((volatile uint32_t *)slots)[h & mask];
+      __threadfence();
+      *s = h + (unsigned long long)mask + 1;
+      return true;
+    }
+  }
+  return false;
+}
+
+// warp-uniform wrappers
+__device__ __forceinline__ bool pool_alloc(const Ctx &c, uint32_t *blk) {
+  const EnumParams &P = *c.P;
+  uint32_t b = 0;
+  bool ok = false;
+  if (c.lane == 0) ok = ring_pop(P.free_slot, P.free_seq, P.free_head, P.free_tail, P.pool_mask, &b, P);
+  ok = __shfl_sync(kFull, ok, 0);
+  *blk = __shfl_sync(kFull, b, 0);
+  return ok;
+}
+
+__device__ __forceinline__ void pool_free(const Ctx &c, uint32_t blk) {
+  const EnumParams &P = *c.P;
+  __syncwarp();
+  if (c.lane == 0) ring_push(P.free_slot, P.free_seq, P.free_tail, P.pool_mask, blk, P);
+  __syncwarp();
+}
+
+__device__ __forceinline__ void pool_publish(const Ctx &c, uint32_t blk) {
+  const EnumParams &P = *c.P;
+  __threadfence();
+  __syncwarp();
+  if (c.lane == 0) {
+    __threadfence();
+    ring_push(P.ready_slot, P.ready_seq, P.ready_tail, P.pool_mask, blk, P);
+    atomicAdd(P.stat_tasks, 1ULL);
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ char *pool_block(const EnumParams &P, uint32_t blk) {
+  return P.pool + (uint64_t)blk * P.block_bytes;
+}
+
+// busy warps expose work when some warps are idle and the queue is short
+__device__ __forceinline__ bool hungry(const Ctx &c) {
+  const EnumParams &P = *c.P;
+  uint32_t h = 0;
+  if (c.lane == 0) {
+    const uint32_t active = *(volatile unsigned int *)P.active;
+    const unsigned long long rh = *(volatile unsigned long long *)P.ready_head;
+    const unsigned long long rt = *(volatile unsigned long long *)P.ready_tail;
+    const uint64_t queued = rt > rh ? rt - rh : 0;
+    const uint32_t idle = P.nwarps > active ? P.nwarps - active : 0;
+    h = idle > 0 && queued < idle;
+  }
+  return __shfl_sync(kFull, h, 0) != 0;
+}
+
+// ------------------------------------------------------- bit compression
+// compress(x, m): the bits of x at the set positions of m, packed to the low
+// end (Hacker's Delight 2nd ed. section 7-4, parallel-suffix form).  The plan
+// depends only on m, which is warp-uniform wherever it is used.
+
+struct CPlan {
+  uint64_t m;
+  uint64_t mv[6];
+};
+
+__device__ __forceinline__ CPlan compress_plan(uint64_t m) {
+  CPlan p;
+  p.m = m;
+  uint64_t mk = ~m << 1;
+#pragma unroll
+  for (int i = 0; i < 6; i++) {
+    uint64_t mp = mk ^ (mk << 1);
+    mp ^= mp << 2;
+    mp ^= mp << 4;
+    mp ^= mp << 8;
+    mp ^= mp << 16;
+    mp ^= mp << 32;
+    const uint64_t mv = mp & m;
+    p.mv[i] = mv;
+    m = (m ^ mv) | (mv >> (1 << i));
+    mk = mk & ~mp;
+  }
+  return p;
+}
+
+__device__ __forceinline__ uint64_t compress_apply(uint64_t x, const CPlan &p) {
+  x &= p.m;
+#pragma unroll
+  for (int i = 0; i < 6; i++) {
+    const uint64_t t = x & p.mv[i];
+    x = (x ^ t) | (t >> (1 << i));
+  }
+  return x;
+}
+
+// multi-word row compaction: out[0..W') = bits of row[0..W) at mask[0..W)
+__device__ __forceinline__ void compress_row(const uint64_t *row, const uint64_t *mask, uint32_t W, uint64_t *out) {
+  uint64_t cur = 0;
+  uint32_t cb = 0, wi = 0;
+  for (uint32_t w = 0; w < W; w++) {
+    const uint64_t m = mask[w];
+    const uint32_t n = __popcll(m);
+    if (n == 0) continue;
+    const uint64_t c = compress_apply(row[w], compress_plan(m));
+    cur |= c << cb;
+    if (cb + n >= 64) {
+      out[wi++] = cur;
+      cur = cb ? (c >> (64 - cb)) : 0;
+      cb = cb + n - 64;
+    } else {
+      cb += n;
+    }
+  }
+  if (cb) out[wi] = cur;
+}
+
+// ---------------------------------------------------------- 32-bit tier
+// At most 32 candidate columns and 32 rows: lane l holds row l as a 32-bit
+// word (rows 0..pc-1 are the column vertices, the rest X rows) plus the label
+// hashes of column l; P, VP and the active-row set are warp-uniform masks.
+
+struct T0 {
+  uint32_t row;
+  uint32_t cv;      // vertex id of column lane
+  uint64_t h1, h2;  // label hashes of column lane
+};
+
+// Child task of candidate q at a 32-bit-tier level, as a W = 1 record.
+__device__ void t0_materialize(const Ctx &c, const T0 &t, uint32_t Pbase, uint32_t A, uint32_t q, uint32_t rsize,
+                               uint64_t s1, uint64_t s2, char *rec) {
+  const uint32_t lane = c.lane;
+  const uint32_t CP = Pbase & __shfl_sync(kFull, t.row, q);
+  const uint32_t pc = __popc(CP);
+  const CPlan plan = compress_plan(CP);
+  const uint64_t hq1 = __shfl_sync(kFull, t.h1, q), hq2 = __shfl_sync(kFull, t.h2, q);
+  uint32_t *colv = (uint32_t *)(rec + kHdr);
+  uint64_t *rows = (uint64_t *)(rec + kHdr + align8(4ULL * pc));
+  const uint64_t cr = compress_apply(t.row, plan);
+  if ((CP >> lane) & 1) {
+    const uint32_t k = __popc(CP & ((1u << lane) - 1));
+    colv[k] = t.cv;
+    rows[k] = cr;
+  }
+  const bool isx = ((A >> lane) & 1) && ((t.row >> q) & 1) && !((CP >> lane) & 1);
+  const uint32_t bal = __ballot_sync(kFull, isx);
+  if (isx) rows[pc + __popc(bal & lanemask_lt())] = cr;
+  if (lane == 0) {
+    TaskHdr *h = (TaskHdr *)rec;
+    h->pc = pc;
+    h->nrows = pc + __popc(bal);
+    h->W = 1;
+    h->rsize = rsize + 1;
+    h->s1 = s1 + hq1;
+    h->s2 = s2 + hq2;
+    h->slot = c.sm->slot;
+  }
+  __syncwarp();
+}
+
+// expose every open candidate of the shallowest open level with |P| >= tau
+// (the reference's TASK_SHARE_BOUND, BkPivotBitBalance.cuh:271-273)
+__device__ void t0_spawn(const Ctx &c, const T0 &t, int level) {
+  WarpSmem *sm = c.sm;
+  int l = 0;
+  uint32_t open = 0;
+  for (; l < level; l++) {
+    const uint4 f = sm->t0f[l];
+    open = f.x & f.y;
+    if (open && (uint32_t)__popc(f.x) + 1 >= c.P->share_bound) break;
+    open = 0;
+  }
+  if (!open) return;
+  const uint4 f = sm->t0f[l];
+  const ulonglong2 hs = sm->t0s[l];
+  uint32_t VPl = f.y;
+  // Highest candidate first: the child of q excludes every open candidate
+  // below q, all still open at that point; whatever stays with this warp is
+  // the lowest candidates, whose children correctly keep the exposed (later)
+  // ones in P.
+  while (open) {
+    const uint32_t q = 31 - __clz(open);
+    open &= ~(1u << q);
+    uint32_t blk;
+    if (!pool_alloc(c, &blk)) break;
+    const uint32_t Pbase = f.x & ~(VPl & ((1u << q) - 1));
+    t0_materialize(c, t, Pbase, f.z, q, f.w, hs.x, hs.y, pool_block(*c.P, blk));
+    pool_publish(c, blk);
+    VPl &= ~(1u << q);
+  }
+  if (c.lane == 0) sm->t0f[l].y = VPl;
+  __syncwarp();
+}
+
+__device__ __noinline__ void t0_solve_body(Ctx c, T0 t, uint32_t pc, uint32_t nrows, uint32_t rsize0, uint64_t s10,
+                                           uint64_t s20) {
+  const uint32_t lane = c.lane;
+  WarpSmem *sm = c.sm;
+  const bool expand_r = c.P->expand_r != 0;
+  uint32_t A = nrows >= 32 ? ~0u : ((1u << nrows) - 1);
+  uint32_t P = pc >= 32 ? ~0u : ((1u << pc) - 1);
+  uint32_t VP = 0, rsize = rsize0;
+  uint64_t s1 = s10, s2 = s20;
+  const uint32_t lanebit = 1u << lane;
+  unsigned long long nodes = 0, wops = 0;  // uniform across lanes
+  int level = 0;
+  bool fresh = true;
+  uint32_t tick = 0;
+  for (;;) {
+    if (fresh) {
+      nodes++;
+      if (P == 0) {
+        if (A == 0 && lane == 0) emit(c, rsize + 2, s1, s2);
+        goto backtrack;
+      }
+      {
+        const uint32_t key = (A & lanebit) ? (((uint32_t)__popc(P & ~t.row) << 5) | lane) : 0xffffffffu;
+        const uint32_t kmin = __reduce_min_sync(kFull, key);
+        wops += 2 * __popc(A);  // ANDN + POPC per active row
+        if ((kmin >> 5) == 0) goto backtrack;  // an X row covers P: nothing maximal below
+        VP = P & ~__shfl_sync(kFull, t.row, kmin & 31);
+        fresh = false;
+      }
+    }
+    {
+      const uint32_t cand = P & VP;
+      if (cand == 0) goto backtrack;
+      const uint32_t q = __ffs(cand) - 1;
+      P &= ~(1u << q);
+      sm->t0f[level] = make_uint4(P, VP, A, rsize);
+      sm->t0s[level] = make_ulonglong2(s1, s2);
+      uint32_t P2 = P & __shfl_sync(kFull, t.row, q);
+      uint64_t n1 = s1 + __shfl_sync(kFull, t.h1, q);
+      uint64_t n2 = s2 + __shfl_sync(kFull, t.h2, q);
+      uint32_t rs = rsize + 1, M = 1u << q;
+      if (expand_r && __popc(P2) > 1) {
+        const bool e = (P2 & lanebit) && __popc(P2 & ~t.row) == 1;
+        const uint32_t E = __ballot_sync(kFull, e);
+        wops += 2 * __popc(P2);
+        if (E) {
+          P2 &= ~E;
+          M |= E;
+          rs += __popc(E);
+          n1 += warp_sum_u64(e ? t.h1 : 0);
+          n2 += warp_sum_u64(e ? t.h2 : 0);
+        }
+      }
+      const uint32_t A2 = A & __ballot_sync(kFull, (t.row & M) == M);
+      wops += __popc(A) + 1;
+      level++;
+      P = P2;
+      VP = 0;
+      A = A2;
+      rsize = rs;
+      s1 = n1;
+      s2 = n2;
+      fresh = true;
+      if (c.sharing && ++tick >= 128) {
+        tick = 0;
+        if (hungry(c)) {
+          const unsigned long long t0 = now();
+          t0_spawn(c, t, level);
+          if (lane == 0) sm->cyc[kCycSpawn] += now() - t0;
+        }
+      }
+      continue;
+    }
+  backtrack:
+    if (level == 0) break;
+    level--;
+    {
+      const uint4 f = sm->t0f[level];
+      const ulonglong2 hs = sm->t0s[level];
+      P = f.x;
+      VP = f.y;
+      A = f.z;
+      rsize = f.w;
+      s1 = hs.x;
+      s2 = hs.y;
+    }
+    fresh = false;
+  }
+  if (lane == 0) {
+    sm->nodes += nodes;
+    sm->wops += wops;
+  }
+  __syncwarp();
+  maybe_flush(c);
+}
+
+// timed wrapper: cycles go to the register-tier phase, spawning excluded
+__device__ __forceinline__ void t0_solve(const Ctx &c, const T0 &t, uint32_t pc, uint32_t nrows, uint32_t rsize0,
+                                         uint64_t s10, uint64_t s20) {
+  const unsigned long long t0 = now(), sp0 = c.sm->cyc[kCycSpawn];
+  t0_solve_body(c, t, pc, nrows, rsize0, s10, s20);
+  if (c.lane == 0) c.sm->cyc[kCycReg] += (now() - t0) - (c.sm->cyc[kCycSpawn] - sp0);
+}
+
+// a W = 1 record with pc <= 32 and nrows <= 32, from a pool block (cg loads)
+// or from this warp's own slab
+template <bool kCoherent>
+__device__ __forceinline__ void t0_load(const Ctx &c, const char *rec, T0 &t, uint32_t pc, uint32_t nrows) {
+  const uint32_t *colv = (const uint32_t *)(rec + kHdr);
+  const uint64_t *rows = (const uint64_t *)(rec + kHdr + align8(4ULL * pc));
+  const uint32_t lane = c.lane;
+  if (kCoherent) {
+    t.row = lane < nrows ? (uint32_t)ld_cg(rows + lane) : 0;
+    t.cv = lane < pc ? ld_cg(colv + lane) : 0;
+  } else {
+    t.row = lane < nrows ? (uint32_t)rows[lane] : 0;
+    t.cv = lane < pc ? colv[lane] : 0;
+  }
+  t.h1 = lane < pc ? c.P->g.h1[t.cv] : 0;
+  t.h2 = lane < pc ? c.P->g.h2[t.cv] : 0;
+}
+
+// ---------------------------------------------------------- 64-bit tier
+
+struct T1 {
+  uint64_t r[kRPL];   // rows lane, lane+32, lane+64, lane+96
+  uint64_t h1a, h1b;  // label hashes of columns lane, lane+32
+  uint64_t h2a, h2b;
+  uint32_t cva, cvb;  // vertex ids of columns lane, lane+32
+};
+
+__device__ __forceinline__ uint64_t sel_row(const T1 &t, uint32_t j) {
+  return j == 0 ? t.r[0] : j == 1 ? t.r[1] : j == 2 ? t.r[2] : t.r[3];
+}
+__device__ __forceinline__ uint64_t bcast_row(const T1 &t, uint32_t idx) {
+  return __shfl_sync(kFull, sel_row(t, idx >> 5), idx & 31);
+}
+
+__device__ __forceinline__ void t1_hashes(const Ctx &c, T1 &t, uint32_t pc) {
+  const DevGraph &g = c.P->g;
+  t.h1a = c.lane < pc ? g.h1[t.cva] : 0;
+  t.h2a = c.lane < pc ? g.h2[t.cva] : 0;
+  t.h1b = c.lane + 32 < pc ? g.h1[t.cvb] : 0;
+  t.h2b = c.lane + 32 < pc ? g.h2[t.cvb] : 0;
+}
+
+// a W = 1 record with nrows <= 128 into registers
+template <bool kCoherent>
+__device__ __forceinline__ void t1_load(const Ctx &c, const char *rec, T1 &t, uint32_t pc, uint32_t nrows) {
+  const uint32_t *colv = (const uint32_t *)(rec + kHdr);
+  const uint64_t *rows = (const uint64_t *)(rec + kHdr + align8(4ULL * pc));
+#pragma unroll
+  for (int j = 0; j < kRPL; j++) {
+    const uint32_t idx = 32 * j + c.lane;
+    t.r[j] = idx < nrows ? (kCoherent ? ld_cg(rows + idx) : rows[idx]) : 0;
+  }
+  t.cva = c.lane < pc ? (kCoherent ? ld_cg(colv + c.lane) : colv[c.lane]) : 0;
+  t.cvb = c.lane + 32 < pc ? (kCoherent ? ld_cg(colv + c.lane + 32) : colv[c.lane + 32]) : 0;
+  t1_hashes(c, t, pc);
+}
+
+// Child task of candidate q of a 64-bit-tier level, into `rec`: columns =
+// Pbase & row(q), rows = active rows holding bit q, compressed to the columns.
+__device__ void t1_materialize(const Ctx &c, const T1 &t, uint64_t Pbase, uint32_t ab, uint32_t q, uint32_t rsize,
+                               uint64_t s1, uint64_t s2, char *rec) {
+  const uint32_t lane = c.lane;
+  const uint64_t CP = Pbase & bcast_row(t, q);
+  const uint32_t pc = __popcll(CP);
+  const CPlan plan = compress_plan(CP);
+  const uint64_t hq1 = __shfl_sync(kFull, q < 32 ? t.h1a : t.h1b, q & 31);
+  const uint64_t hq2 = __shfl_sync(kFull, q < 32 ? t.h2a : t.h2b, q & 31);
+  uint32_t *colv = (uint32_t *)(rec + kHdr);
+  uint64_t *rows = (uint64_t *)(rec + kHdr + align8(4ULL * pc));
+  // candidate rows (row index == column index < 64) in column order
+  if ((CP >> lane) & 1) {
+    const uint32_t k = __popcll(CP & ((1ULL << lane) - 1));
+    colv[k] = t.cva;
+    rows[k] = compress_apply(t.r[0], plan);
+  }
+  if ((CP >> (lane + 32)) & 1) {
+    const uint32_t k = __popcll(CP & ((1ULL << (lane + 32)) - 1));
+    colv[k] = t.cvb;
+    rows[k] = compress_apply(t.r[1], plan);
+  }
+  // X rows: active, holding bit q, not a column of the child
+  uint32_t base = pc;
+#pragma unroll
+  for (int j = 0; j < kRPL; j++) {
+    const uint32_t idx = 32 * j + lane;
+    const bool act = ((ab >> j) & 1) && ((t.r[j] >> q) & 1);
+    const bool isc = idx < 64 && ((CP >> idx) & 1);
+    const bool isx = act && !isc;
+    const uint32_t bal = __ballot_sync(kFull, isx);
+    if (isx) rows[base + __popc(bal & lanemask_lt())] = compress_apply(t.r[j], plan);
+    base += __popc(bal);
+  }
+  if (lane == 0) {
+    TaskHdr *h = (TaskHdr *)rec;
+    h->pc = pc;
+    h->nrows = base;
+    h->W = 1;
+    h->rsize = rsize + 1;
+    h->s1 = s1 + hq1;
+    h->s2 = s2 + hq2;
+    h->slot = c.sm->slot;
+  }
+  __syncwarp();
+}
+
+__device__ void t1_spawn(const Ctx &c, const T1 &t, int level) {
+  WarpSmem *sm = c.sm;
+  int l = 0;
+  uint64_t open = 0;
+  for (; l < level; l++) {
+    open = sm->fP[l] & sm->fVP[l];
+    if (open && (uint32_t)__popcll(sm->fP[l]) + 1 >= c.P->share_bound) break;
+    open = 0;
+  }
+  if (!open) return;
+  const uint64_t Pl = sm->fP[l];
+  uint64_t VPl = sm->fVP[l];
+  const uint32_t abl = sm->fab[l][c.lane];
+  const uint32_t rs = sm->frs[l];
+  const uint64_t s1 = sm->fs1[l], s2 = sm->fs2[l];
+  // highest open candidate first (see t0_spawn)
+  while (open) {
+    const uint32_t q = 63 - __clzll((long long)open);
+    open &= ~(1ULL << q);
+    uint32_t blk;
+    if (!pool_alloc(c, &blk)) break;
+    const uint64_t Pbase = Pl & ~(VPl & ((1ULL << q) - 1));
+    t1_materialize(c, t, Pbase, abl, q, rs, s1, s2, pool_block(*c.P, blk));
+    pool_publish(c, blk);
+    VPl &= ~(1ULL << q);
+  }
+  if (c.lane == 0) sm->fVP[l] = VPl;
+  __syncwarp();
+}
+
+__device__ __noinline__ void t1_solve_body(Ctx c, T1 t, uint32_t pc, uint32_t nrows, uint32_t rsize0, uint64_t s10,
+                                           uint64_t s20) {
+  const uint32_t lane = c.lane;
+  WarpSmem *sm = c.sm;
+  const bool expand_r = c.P->expand_r != 0;
+  uint32_t ab = 0;
+#pragma unroll
+  for (int j = 0; j < kRPL; j++)
+    if (32 * j + lane < nrows) ab |= 1u << j;
+  uint64_t P = pc >= 64 ? ~0ULL : ((1ULL << pc) - 1);
+  uint64_t VP = 0;
+  uint32_t rsize = rsize0;
+  uint64_t s1 = s10, s2 = s20;
+  unsigned long long nodes = 0, wops = 0;  // nodes uniform; wops per lane
+  int level = 0;
+  bool fresh = true;
+  uint32_t tick = 0;
+  for (;;) {
+    if (fresh) {
+      nodes++;
+      if (P == 0) {
+        if (!__any_sync(kFull, ab != 0) && lane == 0) emit(c, rsize + 2, s1, s2);
+        goto backtrack;
+      }
+      {
+        wops += 2 * __popc(ab);
+        uint32_t key = 0xffffffffu;
+#pragma unroll
+        for (int j = 0; j < kRPL; j++)
+          if ((ab >> j) & 1) key = min(key, ((uint32_t)__popcll(P & ~t.r[j]) << 8) | (32 * j + lane));
+        key = __reduce_min_sync(kFull, key);
+        if ((key >> 8) == 0) goto backtrack;  // an X row covers P: nothing maximal below
+        VP = P & ~bcast_row(t, key & 0xff);
+        fresh = false;
+      }
+    }
+    {
+      const uint64_t cand = P & VP;
+      if (cand == 0) goto backtrack;
+      const uint32_t q = __ffsll((long long)cand) - 1;
+      P &= ~(1ULL << q);
+      if (lane == 0) {
+        sm->fP[level] = P;
+        sm->fVP[level] = VP;
+        sm->frs[level] = rsize;
+        sm->fs1[level] = s1;
+        sm->fs2[level] = s2;
+      }
+      sm->fab[level][lane] = (uint8_t)ab;
+      uint64_t P2 = P & bcast_row(t, q);
+      uint64_t n1 = s1 + __shfl_sync(kFull, q < 32 ? t.h1a : t.h1b, q & 31);
+      uint64_t n2 = s2 + __shfl_sync(kFull, q < 32 ? t.h2a : t.h2b, q & 31);
+      uint32_t rs = rsize + 1;
+      uint64_t M = 1ULL << q;
+      if (expand_r && __popcll(P2) > 1) {
+        wops += 2 * (((P2 >> lane) & 1) + ((P2 >> (lane + 32)) & 1));
+        const bool e0 = ((P2 >> lane) & 1) && __popcll(P2 & ~t.r[0]) == 1;
+        const bool e1 = ((P2 >> (lane + 32)) & 1) && __popcll(P2 & ~t.r[1]) == 1;
+        const uint64_t E = (uint64_t)__ballot_sync(kFull, e0) | ((uint64_t)__ballot_sync(kFull, e1) << 32);
+        if (E) {
+          P2 &= ~E;
+          M |= E;
+          rs += __popcll(E);
+          n1 += warp_sum_u64((e0 ? t.h1a : 0) + (e1 ? t.h1b : 0));
+          n2 += warp_sum_u64((e0 ? t.h2a : 0) + (e1 ? t.h2b : 0));
+        }
+      }
+      uint32_t ab2 = 0;
+#pragma unroll
+      for (int j = 0; j < kRPL; j++)
+        if (((ab >> j) & 1) && (t.r[j] & M) == M) ab2 |= 1u << j;
+      wops += __popc(ab) + (lane == 0 ? 1 : 0);
+      // A child with <= 32 columns and <= 32 active rows drops to the 32-bit
+      // tier: rows compressed to the child's columns and gathered, columns
+      // first, through the warp's exchange buffer.
+      const uint32_t nact = __reduce_add_sync(kFull, __popc(ab2));
+      if (__popcll(P2) <= 32 && nact <= 32) {
+        const uint32_t pc2 = __popcll(P2);
+        const CPlan plan = compress_plan(P2);
+        uint32_t base = pc2;
+#pragma unroll
+        for (int j = 0; j < kRPL; j++) {
+          const uint32_t idx = 32 * j + lane;
+          const bool act = (ab2 >> j) & 1;
+          const bool isc = idx < 64 && ((P2 >> idx) & 1);
+          if (act && isc) {
+            const uint32_t k = __popcll(P2 & ((1ULL << idx) - 1));
+            sm->xrow[k] = (uint32_t)compress_apply(t.r[j], plan);
+            sm->xcv[k] = j == 0 ? t.cva : t.cvb;
+            sm->xh1[k] = j == 0 ? t.h1a : t.h1b;
+            sm->xh2[k] = j == 0 ? t.h2a : t.h2b;
+          }
+          const bool isx = act && !isc;
+          const uint32_t bal = __ballot_sync(kFull, isx);
+          if (isx) sm->xrow[base + __popc(bal & lanemask_lt())] = (uint32_t)compress_apply(t.r[j], plan);
+          base += __popc(bal);
+        }
+        __syncwarp();
+        T0 t0;
+        t0.row = lane < nact ? sm->xrow[lane] : 0;
+        t0.cv = lane < pc2 ? sm->xcv[lane] : 0;
+        t0.h1 = lane < pc2 ? sm->xh1[lane] : 0;
+        t0.h2 = lane < pc2 ? sm->xh2[lane] : 0;
+        __syncwarp();
+        t0_solve_body(c, t0, pc2, nact, rs, n1, n2);
+        continue;  // next candidate at this level
+      }
+      level++;
+      P = P2;
+      VP = 0;
+      rsize = rs;
+      s1 = n1;
+      s2 = n2;
+      ab = ab2;
+      fresh = true;
+      if (c.sharing && ++tick >= 64) {
+        tick = 0;
+        if (hungry(c)) {
+          const unsigned long long t0 = now();
+          t1_spawn(c, t, level);
+          if (lane == 0) sm->cyc[kCycSpawn] += now() - t0;
+        }
+      }
+      continue;
+    }
+  backtrack:
+    if (level == 0) break;
+    level--;
+    P = sm->fP[level];
+    VP = sm->fVP[level];
+    rsize = sm->frs[level];
+    s1 = sm->fs1[level];
+    s2 = sm->fs2[level];
+    ab = sm->fab[level][lane];
+    fresh = false;
+  }
+  wops = warp_sum_u64(wops);
+  if (lane == 0) {
+    sm->nodes += nodes;
+    sm->wops += wops;
+  }
+  __syncwarp();
+  maybe_flush(c);
+}
+
+__device__ __forceinline__ void t1_solve(const Ctx &c, const T1 &t, uint32_t pc, uint32_t nrows, uint32_t rsize0,
+                                         uint64_t s10, uint64_t s20) {
+  const unsigned long long t0 = now(), sp0 = c.sm->cyc[kCycSpawn];
+  t1_solve_body(c, t, pc, nrows, rsize0, s10, s20);
+  if (c.lane == 0) c.sm->cyc[kCycReg] += (now() - t0) - (c.sm->cyc[kCycSpawn] - sp0);
+}
+
+// a register-tier record (W == 1) in this warp's own slab
+__device__ void reg_from_local(const Ctx &c, const char *rec) {
+  const TaskHdr *h = (const TaskHdr *)rec;
+  const uint32_t pc = h->pc, nrows = h->nrows, rsize = h->rsize;
+  const uint64_t s1 = h->s1, s2 = h->s2;
+  if (pc <= 32 && nrows <= 32) {
+    T0 t0;
+    t0_load<false>(c, rec, t0, pc, nrows);
+    __syncwarp();
+    t0_solve(c, t0, pc, nrows, rsize, s1, s2);
+    return;
+  }
+  T1 t;
+  t1_load<false>(c, rec, t, pc, nrows);
+  __syncwarp();
+  t1_solve(c, t, pc, nrows, rsize, s1, s2);
+}
+
+// --------------------------------------------------------- general tier
+
+struct Gen {
+  const uint64_t *rows;
+  const uint32_t *colv;
+  const uint64_t *h1s, *h2s;
+  uint64_t *stack;
+  uint32_t *alist;
+  uint64_t alist_cap;
+  uint32_t pc, nrows, W;
+};
+
+// Child of candidate q at a general-tier level (record rec_l) as a task
+// record in `out`: columns = Pbase & row(q), rows = active rows holding bit q
+// (and all of R' when the level's list is inherited), compressed to the child
+// columns.  Returns false when the record would exceed max_bytes.
+__device__ bool gen_materialize(const Ctx &c, const Gen &G, const uint64_t *rec_l, uint32_t q,
+                                const uint64_t *Pbase, uint64_t max_bytes, char *out) {
+  const uint32_t lane = c.lane, W = G.W;
+  uint64_t *CP = c.sm->rowbuf;
+  const uint64_t *rowq = G.rows + (uint64_t)q * W;
+  uint32_t pc = 0;
   for (uint32_t w = lane; w < W; w += 32) {
-    uint32_t lo = w * 64;
-    stack[w] = (p - lo >= 64) ? ~0ULL : ((1ULL << (p - lo)) - 1);
+    const uint64_t v = Pbase[w] & rowq[w];
+    CP[w] = v;
+    pc += __popcll(v);
+  }
+  pc = __reduce_add_sync(kFull, pc);
+  __syncwarp();
+  const uint32_t Wn = (pc + 63) / 64;
+  const uint64_t m0 = rec_l[3 * W], m1 = rec_l[3 * W + 1];
+  const uint32_t aoff = (uint32_t)m0, alen = (uint32_t)(m0 >> 32);
+  const bool lazy = (m1 >> 63) != 0;
+  const uint64_t *R = rec_l + 2 * W;
+  const uint32_t wq = q >> 6;
+  const uint64_t bq = 1ULL << (q & 63);
+  auto keep_row = [&](uint32_t i) -> bool {
+    const uint64_t *row = G.rows + (uint64_t)i * W;
+    if (!(row[wq] & bq)) return false;
+    if (lazy)
+      for (uint32_t w = 0; w < W; w++)
+        if ((R[w] & row[w]) != R[w]) return false;
+    return true;
+  };
+  auto is_col = [&](uint32_t i) -> bool { return i < G.pc && ((CP[i >> 6] >> (i & 63)) & 1); };
+  uint32_t nx = 0;
+  for (uint32_t base = 0; base < alen; base += 32) {
+    const uint32_t t = base + lane;
+    bool x = false;
+    if (t < alen) {
+      const uint32_t i = aoff == kIdent ? t : G.alist[aoff + t];
+      x = !is_col(i) && keep_row(i);
+    }
+    nx += __popc(__ballot_sync(kFull, x));
+  }
+  const uint32_t nrows = pc + nx;
+  if (task_bytes(pc, nrows, Wn) > max_bytes) return false;
+  uint32_t *colv = (uint32_t *)(out + kHdr);
+  uint64_t *rows = (uint64_t *)(out + kHdr + align8(4ULL * pc));
+  // child columns: parent candidate rows i < pc with CP bit i, in order
+  for (uint32_t i = lane; i < G.pc; i += 32) {
+    if (is_col(i)) {
+      uint32_t k = 0;
+      for (uint32_t w = 0; w < (i >> 6); w++) k += __popcll(CP[w]);
+      k += __popcll(CP[i >> 6] & ((1ULL << (i & 63)) - 1));
+      colv[k] = G.colv[i];
+      compress_row(G.rows + (uint64_t)i * W, CP, W, rows + (uint64_t)k * Wn);
+    }
+  }
+  uint32_t pos = pc;
+  for (uint32_t base = 0; base < alen; base += 32) {
+    const uint32_t t = base + lane;
+    bool x = false;
+    uint32_t i = 0;
+    if (t < alen) {
+      i = aoff == kIdent ? t : G.alist[aoff + t];
+      x = !is_col(i) && keep_row(i);
+    }
+    const uint32_t bal = __ballot_sync(kFull, x);
+    if (x) compress_row(G.rows + (uint64_t)i * W, CP, W, rows + (uint64_t)(pos + __popc(bal & lanemask_lt())) * Wn);
+    pos += __popc(bal);
+  }
+  if (lane == 0) {
+    TaskHdr *h = (TaskHdr *)out;
+    h->pc = pc;
+    h->nrows = nrows;
+    h->W = Wn;
+    h->rsize = ((uint32_t)(m1 >> 32) & 0x7fffffffu) + 1;
+    h->s1 = rec_l[3 * W + 2] + G.h1s[q];
+    h->s2 = rec_l[3 * W + 3] + G.h2s[q];
+    h->slot = c.sm->slot;
+  }
+  __syncwarp();
+  return true;
+}
+
+__device__ void gen_spawn(const Ctx &c, const Gen &G, int level) {
+  const uint32_t W = G.W, lane = c.lane;
+  const uint64_t LREC = 3ULL * W + 4;
+  int l = -1;
+  for (int k = 0; k < level && l < 0; k++) {
+    const uint64_t *rec = G.stack + (uint64_t)k * LREC;
+    bool any = false;
+    uint32_t pc = 0;
+    for (uint32_t w = lane; w < W; w += 32) {
+      any |= (rec[w] & rec[W + w]) != 0;
+      pc += __popcll(rec[w]);
+    }
+    pc = __reduce_add_sync(kFull, pc);
+    if (__any_sync(kFull, any) && pc + 1 >= c.P->share_bound) l = k;
+  }
+  if (l < 0) return;
+  uint64_t *rec = G.stack + (uint64_t)l * LREC;
+  uint64_t *Pl = rec, *VPl = rec + W;
+  // scratch record past the deepest level holds Pbase
+  uint64_t *Pbase = G.stack + (uint64_t)(G.pc + 2) * LREC;
+  // highest open candidate first (see t0_spawn)
+  uint32_t spawned = 0;
+  for (int wq = (int)W - 1; wq >= 0 && spawned < 256; wq--) {
+    for (;;) {
+      const uint64_t open = Pl[wq] & VPl[wq];
+      if (!open) break;
+      const uint32_t q = wq * 64 + (63 - __clzll((long long)open));
+      uint32_t blk;
+      if (!pool_alloc(c, &blk)) return;
+      for (uint32_t w = lane; w < W; w += 32) {
+        const uint64_t below = (int)w < wq ? ~0ULL : ((int)w == wq ? ((1ULL << (q & 63)) - 1) : 0);
+        Pbase[w] = Pl[w] & ~(VPl[w] & below);
+      }
+      __syncwarp();
+      const bool ok = gen_materialize(c, G, rec, q, Pbase, c.P->block_bytes, pool_block(*c.P, blk));
+      if (!ok) {
+        pool_free(c, blk);
+        return;
+      }
+      pool_publish(c, blk);
+      if (lane == 0) VPl[wq] &= ~(1ULL << (q & 63));
+      __syncwarp();
+      spawned++;
+    }
+  }
+}
+
+// Solve a general-tier ego network laid out in the slab.
+__device__ __noinline__ void gen_solve_body(Ctx c, Gen G, uint32_t rsize0, uint64_t s10, uint64_t s20) {
+  const uint32_t lane = c.lane, W = G.W;
+  WarpSmem *sm = c.sm;
+  const uint64_t LREC = 3ULL * W + 4;
+  uint64_t *stack = G.stack;
+  uint32_t *alist = G.alist;
+  const uint64_t *rows = G.rows;
+  char *local = c.slab + c.slab_bytes - kLocalRec;
+  unsigned long long nodes = 0, wops = 0;
+  for (uint32_t w = lane; w < W; w += 32) {
+    const uint32_t lo = w * 64;
+    stack[w] = (G.pc - lo >= 64) ? ~0ULL : ((1ULL << (G.pc - lo)) - 1);
     stack[W + w] = 0;
     stack[2 * W + w] = 0;
   }
   if (lane == 0) {
     uint64_t *m = stack + 3 * W;
-    m[0] = (uint64_t)kIdent | ((uint64_t)nrows << 32);
-    m[1] = 0;  // atop 0, rsize 0, not lazy
-    m[2] = s1_root;
-    m[3] = s2_root;
+    m[0] = (uint64_t)kIdent | ((uint64_t)G.nrows << 32);
+    m[1] = (uint64_t)rsize0 << 32;
+    m[2] = s10;
+    m[3] = s20;
   }
   __syncwarp();
   int level = 0;
   bool fresh = true;
+  uint32_t tick = 0;
   for (;;) {
     uint64_t *rec = stack + (uint64_t)level * LREC;
     uint64_t *Pv = rec, *VP = rec + W, *R = rec + 2 * W;
@@ -131,58 +992,50 @@ __device__ void solve_ego(const EnumParams &P, WarpAcc &acc, uint32_t *hcache, c
     const uint32_t atop = (uint32_t)m1, rsize = (uint32_t)(m1 >> 32) & 0x7fffffffu;
     const bool lazy = (m1 >> 63) != 0;
     if (fresh) {
-      uint32_t pc = 0;
-      for (uint32_t w = lane; w < W; w += 32) pc += __popcll(Pv[w]);
-      pc = __reduce_add_sync(kFull, pc);
-      if (pc == 0) {
-        // leaf: maximal iff no active row contains R
+      nodes++;
+      uint32_t pcnt = 0;
+      for (uint32_t w = lane; w < W; w += 32) pcnt += __popcll(Pv[w]);
+      pcnt = __reduce_add_sync(kFull, pcnt);
+      if (pcnt == 0) {
         bool blocked;
         if (!lazy) {
           blocked = alen > 0;
         } else {
           bool hit = false;
           for (uint32_t base = 0; base < alen && !hit; base += 32) {
-            uint32_t t = base + lane;
+            const uint32_t t = base + lane;
             bool h = false;
             if (t < alen) {
-              uint32_t i = aoff == kIdent ? t : alist[aoff + t];
+              const uint32_t i = aoff == kIdent ? t : alist[aoff + t];
               const uint64_t *row = rows + (uint64_t)i * W;
               h = true;
-              for (uint32_t w = 0; w < W; w++)
-                if (R[w] & ~row[w]) {
-                  h = false;
-                  break;
-                }
+              for (uint32_t w = 0; w < W && h; w++) h = (R[w] & ~row[w]) == 0;
             }
             hit = __any_sync(kFull, h);
           }
           blocked = hit;
         }
-        if (!blocked && lane == 0) emit(P, acc, hcache, rsize + 2, rec[3 * W + 2], rec[3 * W + 3]);
+        if (!blocked && lane == 0) emit(c, rsize + 2, rec[3 * W + 2], rec[3 * W + 3]);
         fresh = false;
         if (level == 0) break;
         level--;
         continue;
       }
-      // pivot scan over active rows
       uint32_t best_c = 0xffffffffu, best_t = 0xffffffffu;
       for (uint32_t base = 0; base < alen; base += 32) {
-        uint32_t t = base + lane;
+        const uint32_t t = base + lane;
         if (t < alen) {
-          uint32_t i = aoff == kIdent ? t : alist[aoff + t];
+          const uint32_t i = aoff == kIdent ? t : alist[aoff + t];
           const uint64_t *row = rows + (uint64_t)i * W;
           bool ok = true;
           if (lazy)
-            for (uint32_t w = 0; w < W; w++)
-              if (R[w] & ~row[w]) {
-                ok = false;
-                break;
-              }
+            for (uint32_t w = 0; w < W && ok; w++) ok = (R[w] & ~row[w]) == 0;
           if (ok) {
-            uint32_t c = 0;
-            for (uint32_t w = 0; w < W; w++) c += __popcll(Pv[w] & ~row[w]);
-            if (c < best_c) {
-              best_c = c;
+            uint32_t cnt = 0;
+            wops += 2 * W;
+            for (uint32_t w = 0; w < W; w++) cnt += __popcll(Pv[w] & ~row[w]);
+            if (cnt < best_c) {
+              best_c = cnt;
               best_t = t;
             }
           }
@@ -191,7 +1044,6 @@ __device__ void solve_ego(const EnumParams &P, WarpAcc &acc, uint32_t *hcache, c
       }
       const uint32_t minc = __reduce_min_sync(kFull, best_c);
       if (minc == 0 || minc == 0xffffffffu) {
-        // an X row adjacent to all of P: nothing maximal below this node
         fresh = false;
         if (level == 0) break;
         level--;
@@ -203,17 +1055,16 @@ __device__ void solve_ego(const EnumParams &P, WarpAcc &acc, uint32_t *hcache, c
       for (uint32_t w = lane; w < W; w += 32) VP[w] = Pv[w] & ~prow[w];
       __syncwarp();
       fresh = false;
-      continue;  // pick the first candidate at this level
+      continue;
     }
-    // next candidate at this level: first bit of P & VP
     uint32_t q = 0xffffffffu;
     for (uint32_t wb = 0; wb < W; wb += 32) {
-      uint32_t w = wb + lane;
-      uint64_t val = w < W ? (Pv[w] & VP[w]) : 0;
-      uint32_t bal = __ballot_sync(kFull, val != 0);
+      const uint32_t w = wb + lane;
+      const uint64_t val = w < W ? (Pv[w] & VP[w]) : 0;
+      const uint32_t bal = __ballot_sync(kFull, val != 0);
       if (bal) {
-        uint32_t src = __ffs(bal) - 1;
-        uint64_t vv = __shfl_sync(kFull, val, src);
+        const uint32_t src = __ffs(bal) - 1;
+        const uint64_t vv = __shfl_sync(kFull, val, src);
         q = (wb + src) * 64 + (__ffsll((long long)vv) - 1);
         break;
       }
@@ -227,13 +1078,12 @@ __device__ void solve_ego(const EnumParams &P, WarpAcc &acc, uint32_t *hcache, c
     const uint64_t bq = 1ULL << (q & 63);
     if (lane == 0) Pv[wq] &= ~bq;
     __syncwarp();
-    // child node
     uint64_t *crec = rec + LREC;
     uint64_t *CP = crec, *CE = crec + W, *CR = crec + 2 * W;
     const uint64_t *rowq = rows + (uint64_t)q * W;
     uint32_t cpc = 0;
     for (uint32_t w = lane; w < W; w += 32) {
-      uint64_t cp = Pv[w] & rowq[w];
+      const uint64_t cp = Pv[w] & rowq[w];
       CP[w] = cp;
       CR[w] = R[w] | (w == wq ? bq : 0);
       CE[w] = 0;
@@ -241,27 +1091,58 @@ __device__ void solve_ego(const EnumParams &P, WarpAcc &acc, uint32_t *hcache, c
     }
     cpc = __reduce_add_sync(kFull, cpc);
     __syncwarp();
+    // a child small enough for the register tiers leaves the general tier here
+    if (cpc <= 64 && cpc > 0) {
+      uint32_t ccount = 0;
+      for (uint32_t base = 0; base < alen; base += 32) {
+        const uint32_t t = base + lane;
+        bool keep = false;
+        if (t < alen) {
+          const uint32_t i = aoff == kIdent ? t : alist[aoff + t];
+          const uint64_t *row = rows + (uint64_t)i * W;
+          keep = (row[wq] & bq) != 0;
+          if (lazy)
+            for (uint32_t w = 0; w < W && keep; w++) keep = (R[w] & row[w]) == R[w];
+        }
+        ccount += __popc(__ballot_sync(kFull, keep));
+      }
+      if (ccount <= kT1Rows && gen_materialize(c, G, rec, q, Pv, kLocalRec, local)) {
+        const unsigned long long t0 = now(), sp0 = sm->cyc[kCycSpawn];
+        reg_from_local(c, local);
+        // the register-tier time is booked there; keep it out of this phase
+        if (lane == 0) sm->cyc[kCycGen] -= (now() - t0) - (sm->cyc[kCycSpawn] - sp0);
+        if (c.sharing && ++tick >= 8) {
+          tick = 0;
+          if (hungry(c)) {
+            const unsigned long long ts = now();
+            gen_spawn(c, G, level + 1);
+            if (lane == 0) sm->cyc[kCycSpawn] += now() - ts;
+          }
+        }
+        continue;  // next candidate at this level
+      }
+    }
     uint32_t rs = rsize + 1;
-    uint64_t t1 = rec[3 * W + 2] + h1s[q], t2 = rec[3 * W + 3] + h2s[q];
+    uint64_t t1 = rec[3 * W + 2] + G.h1s[q], t2 = rec[3 * W + 3] + G.h2s[q];
     uint32_t nE = 0;
-    if (P.expand_r && cpc > 1) {
+    if (c.P->expand_r && cpc > 1) {
       uint64_t e1 = 0, e2 = 0;
       uint32_t ne = 0;
-      for (uint32_t base = 0; base < p; base += 32) {
-        uint32_t i = base + lane;
+      for (uint32_t base = 0; base < G.pc; base += 32) {
+        const uint32_t i = base + lane;
         bool e = false;
-        if (i < p && ((CP[i >> 6] >> (i & 63)) & 1)) {
+        if (i < G.pc && ((CP[i >> 6] >> (i & 63)) & 1)) {
           const uint64_t *ri = rows + (uint64_t)i * W;
-          uint32_t c = 0;
-          for (uint32_t w = 0; w < W && c <= 1; w++) c += __popcll(CP[w] & ~ri[w]);
-          e = (c == 1);
+          uint32_t cc = 0;
+          for (uint32_t w = 0; w < W && cc <= 1; w++) cc += __popcll(CP[w] & ~ri[w]);
+          e = (cc == 1);
         }
-        uint32_t bal = __ballot_sync(kFull, e);
+        const uint32_t bal = __ballot_sync(kFull, e);
         if (bal) {
           if (lane == 0) CE[base >> 6] |= (uint64_t)bal << (base & 32);
           if (e) {
-            e1 += h1s[i];
-            e2 += h2s[i];
+            e1 += G.h1s[i];
+            e2 += G.h2s[i];
             ne++;
           }
         }
@@ -272,7 +1153,7 @@ __device__ void solve_ego(const EnumParams &P, WarpAcc &acc, uint32_t *hcache, c
         e2 = warp_sum_u64(e2);
         __syncwarp();
         for (uint32_t w = lane; w < W; w += 32) {
-          uint64_t ew = CE[w];
+          const uint64_t ew = CE[w];
           CP[w] &= ~ew;
           CR[w] |= ew;
         }
@@ -282,30 +1163,26 @@ __device__ void solve_ego(const EnumParams &P, WarpAcc &acc, uint32_t *hcache, c
       }
     }
     __syncwarp();
-    // child active rows
     uint32_t caoff, calen, catop;
     bool clazy;
-    if ((uint64_t)atop + alen <= alist_cap) {
+    if ((uint64_t)atop + alen <= G.alist_cap) {
       uint32_t n2 = 0;
       const bool single = !lazy && nE == 0;
       for (uint32_t base = 0; base < alen; base += 32) {
-        uint32_t t = base + lane;
+        const uint32_t t = base + lane;
         bool keep = false;
         uint32_t i = 0;
         if (t < alen) {
+          wops += single ? 1 : W;
           i = aoff == kIdent ? t : alist[aoff + t];
           const uint64_t *row = rows + (uint64_t)i * W;
-          if (single) {
-            keep = (row[wq] & bq) != 0;
-          } else if (!lazy) {
-            keep = (row[wq] & bq) != 0;
-            for (uint32_t w = 0; w < W && keep; w++) keep = (row[w] & CE[w]) == CE[w];
-          } else {
-            keep = true;
-            for (uint32_t w = 0; w < W && keep; w++) keep = (row[w] & CR[w]) == CR[w];
+          keep = (row[wq] & bq) != 0;
+          if (!single) {
+            const uint64_t *need = lazy ? CR : CE;
+            for (uint32_t w = 0; w < W && keep; w++) keep = (row[w] & need[w]) == need[w];
           }
         }
-        uint32_t bal = __ballot_sync(kFull, keep);
+        const uint32_t bal = __ballot_sync(kFull, keep);
         if (keep) alist[atop + n2 + __popc(bal & lanemask_lt())] = i;
         n2 += __popc(bal);
       }
@@ -328,11 +1205,33 @@ __device__ void solve_ego(const EnumParams &P, WarpAcc &acc, uint32_t *hcache, c
     __syncwarp();
     level++;
     fresh = true;
+    if (c.sharing && ++tick >= 8) {
+      tick = 0;
+      if (hungry(c)) {
+        const unsigned long long ts = now();
+        gen_spawn(c, G, level);
+        if (lane == 0) sm->cyc[kCycSpawn] += now() - ts;
+      }
+    }
   }
+  wops = warp_sum_u64(wops);
+  if (lane == 0) {
+    sm->nodes += nodes;
+    sm->wops += wops;
+  }
+  __syncwarp();
+  maybe_flush(c);
 }
 
-// Candidate list C = N(v0) & N(v1) (sorted) into cand[]; returns |C| or
-// 0xffffffff if more than cap.
+__device__ __forceinline__ void gen_solve(const Ctx &c, const Gen &G, uint32_t rsize0, uint64_t s10, uint64_t s20) {
+  const unsigned long long t0 = now(), sp0 = c.sm->cyc[kCycSpawn];
+  gen_solve_body(c, G, rsize0, s10, s20);
+  if (c.lane == 0) c.sm->cyc[kCycGen] += (now() - t0) - (c.sm->cyc[kCycSpawn] - sp0);
+}
+
+// ------------------------------------------------------------ root build
+
+// C = N(v0) & N(v1) (sorted) into cand[]; |C|, or 0xffffffff beyond cap
 __device__ uint32_t intersect(const DevGraph &g, uint32_t v0, uint32_t v1, uint32_t *cand, uint64_t cap) {
   const uint32_t lane = lane_id();
   const uint32_t *a = g.adj + g.off[v0], *b = g.adj + g.off[v1];
@@ -341,16 +1240,16 @@ __device__ uint32_t intersect(const DevGraph &g, uint32_t v0, uint32_t v1, uint3
     const uint32_t *t = a;
     a = b;
     b = t;
-    uint32_t td = da;
+    const uint32_t td = da;
     da = db;
     db = td;
   }
   uint32_t nc = 0;
   for (uint32_t base = 0; base < da; base += 32) {
-    uint32_t t = base + lane;
-    uint32_t val = t < da ? __ldg(a + t) : 0;
-    bool hit = t < da && val != v0 && val != v1 && contains_u32(b, db, val);
-    uint32_t bal = __ballot_sync(kFull, hit);
+    const uint32_t t = base + lane;
+    const uint32_t val = t < da ? __ldg(a + t) : 0;
+    const bool hit = t < da && contains_u32(b, db, val);
+    const uint32_t bal = __ballot_sync(kFull, hit);
     if (nc + __popc(bal) > cap) return 0xffffffffu;
     if (hit) cand[nc + __popc(bal & lanemask_lt())] = val;
     nc += __popc(bal);
@@ -359,8 +1258,7 @@ __device__ uint32_t intersect(const DevGraph &g, uint32_t v0, uint32_t v1, uint3
   return nc;
 }
 
-// Build the ego bitmap.  Returns number of rows kept (P rows + X rows with a
-// P neighbour).  rowbuf: per-warp shared buffer of 64 words.
+// Ego bitmap rows (candidate rows, then X rows with a candidate neighbour).
 __device__ uint32_t build_rows(const DevGraph &g, const uint32_t *cand, uint32_t x, uint32_t p, uint32_t W,
                                uint64_t *rows, uint64_t *rowbuf) {
   const uint32_t lane = lane_id();
@@ -372,7 +1270,6 @@ __device__ uint32_t build_rows(const DevGraph &g, const uint32_t *cand, uint32_t
     const uint32_t *nu = g.adj + g.off[u];
     const uint32_t du = g.off[u + 1] - g.off[u];
     uint64_t *row = rows + (uint64_t)nrows * W;
-    // restrict N(u) to [pmin, pmax]
     uint32_t lo = 0, hi = 0;
     if (lane == 0) {
       lo = lower_bound_u32(nu, du, pmin);
@@ -382,13 +1279,12 @@ __device__ uint32_t build_rows(const DevGraph &g, const uint32_t *cand, uint32_t
     hi = __shfl_sync(kFull, hi, 0);
     bool any;
     if (hi - lo < p && W <= 64) {
-      // lanes over N(u) slice, binary search in P, OR into shared row
       for (uint32_t w = lane; w < W; w += 32) rowbuf[w] = 0;
       __syncwarp();
       bool hit = false;
       for (uint32_t e = lo + lane; e < hi; e += 32) {
-        uint32_t y = __ldg(nu + e);
-        uint32_t j = lower_bound_u32(Pl, p, y);
+        const uint32_t y = __ldg(nu + e);
+        const uint32_t j = lower_bound_u32(Pl, p, y);
         if (j < p && Pl[j] == y) {
           atomicOr((unsigned long long *)&rowbuf[j >> 6], 1ULL << (j & 63));
           hit = true;
@@ -398,15 +1294,14 @@ __device__ uint32_t build_rows(const DevGraph &g, const uint32_t *cand, uint32_t
       __syncwarp();
       for (uint32_t w = lane; w < W; w += 32) row[w] = rowbuf[w];
     } else {
-      // lanes over P, binary search in the N(u) slice
       uint64_t word = 0;
       bool hitany = false;
       const uint32_t *sl = nu + lo;
       const uint32_t sn = hi - lo;
       for (uint32_t base = 0; base < p; base += 32) {
-        uint32_t j = base + lane;
-        bool hit = j < p && contains_u32(sl, sn, Pl[j]);
-        uint32_t bal = __ballot_sync(kFull, hit);
+        const uint32_t j = base + lane;
+        const bool hit = j < p && contains_u32(sl, sn, Pl[j]);
+        const uint32_t bal = __ballot_sync(kFull, hit);
         hitany |= bal != 0;
         if (base & 32) {
           word |= (uint64_t)bal << 32;
@@ -424,105 +1319,337 @@ __device__ uint32_t build_rows(const DevGraph &g, const uint32_t *cand, uint32_t
   return nrows;
 }
 
-__global__ void __launch_bounds__(256, 2) k_enumerate(EnumParams P) {
-  extern __shared__ uint64_t smem[];
-  const uint32_t lane = lane_id();
-  const uint32_t wib = threadIdx.x >> 5;
+// Slab layout of a general-tier problem (bytes from the slab start).
+struct Layout {
+  uint64_t colv_off, hash_off, rows_off, stack_off, alist_off, need;
+};
+
+__host__ __device__ __forceinline__ Layout layout_for(uint64_t cand_n, uint32_t pc, uint32_t nrows, uint32_t W) {
+  Layout L;
+  L.colv_off = 0;
+  L.hash_off = align8(4ULL * cand_n);
+  L.rows_off = L.hash_off + 16ULL * pc;
+  L.stack_off = L.rows_off + 8ULL * (uint64_t)nrows * W;
+  // pc + 1 levels, one scratch record past the deepest, one spare
+  L.alist_off = L.stack_off + 8ULL * (uint64_t)(pc + 3) * (3ULL * W + 4);
+  L.need = L.alist_off + 4ULL * nrows + kLocalRec;
+  return L;
+}
+
+// Solve root r.  Returns false when the root does not fit this slab.
+__device__ bool solve_root(const Ctx &c, uint64_t r) {
+  const DevGraph &g = c.P->g;
+  const uint32_t v0 = g.root_v0[r], v1 = g.root_v1[r];
+  set_slot(c, g.slot ? g.slot[v0] : 0);
+  uint32_t *cand = (uint32_t *)c.slab;
+  const uint64_t cap = (c.slab_bytes - kLocalRec) / 4;
+  const unsigned long long tb0 = now();
+  const uint32_t nc = intersect(g, v0, v1, cand, cap);
+  if (nc == 0xffffffffu) {
+    if (c.lane == 0) c.sm->cyc[kCycBuild] += now() - tb0;
+    return false;
+  }
+  const uint32_t x = nc ? lower_bound_u32(cand, nc, v1) : 0;
+  const uint32_t p = nc - x;
+  const uint64_t s1 = g.h1[v0] + g.h1[v1], s2 = g.h2[v0] + g.h2[v1];
+  if (p == 0) {
+    if (x == 0 && c.lane == 0) emit(c, 2, s1, s2);
+    if (c.lane == 0) c.sm->cyc[kCycBuild] += now() - tb0;
+    return true;
+  }
+  const uint32_t W = (p + 63) / 64;
+  const Layout L = layout_for(nc, p, p + x, W);
+  if (L.need > c.slab_bytes) {
+    if (c.lane == 0) c.sm->cyc[kCycBuild] += now() - tb0;
+    return false;
+  }
+  uint64_t *rows = (uint64_t *)(c.slab + L.rows_off);
+  const uint32_t nrows = build_rows(g, cand, x, p, W, rows, c.sm->rowbuf);
+  __syncwarp();
+  if (c.lane == 0) c.sm->cyc[kCycBuild] += now() - tb0;
+  if (p <= 32 && nrows <= 32) {
+    T0 t0;
+    t0.row = c.lane < nrows ? (uint32_t)rows[c.lane] : 0;
+    t0.cv = c.lane < p ? cand[x + c.lane] : 0;
+    t0.h1 = c.lane < p ? g.h1[t0.cv] : 0;
+    t0.h2 = c.lane < p ? g.h2[t0.cv] : 0;
+    __syncwarp();
+    t0_solve(c, t0, p, nrows, 0, s1, s2);
+    return true;
+  }
+  if (W == 1 && nrows <= kT1Rows) {
+    T1 t;
+#pragma unroll
+    for (int j = 0; j < kRPL; j++) {
+      const uint32_t idx = 32 * j + c.lane;
+      t.r[j] = idx < nrows ? rows[idx] : 0;
+    }
+    t.cva = c.lane < p ? cand[x + c.lane] : 0;
+    t.cvb = c.lane + 32 < p ? cand[x + c.lane + 32] : 0;
+    t1_hashes(c, t, p);
+    __syncwarp();
+    t1_solve(c, t, p, nrows, 0, s1, s2);
+    return true;
+  }
+  Gen G;
+  G.rows = rows;
+  G.colv = cand + x;
+  uint64_t *h1s = (uint64_t *)(c.slab + L.hash_off);
+  uint64_t *h2s = h1s + p;
+  for (uint32_t j = c.lane; j < p; j += 32) {
+    const uint32_t y = cand[x + j];
+    h1s[j] = g.h1[y];
+    h2s[j] = g.h2[y];
+  }
+  G.h1s = h1s;
+  G.h2s = h2s;
+  G.stack = (uint64_t *)(c.slab + L.stack_off);
+  G.alist = (uint32_t *)(c.slab + L.alist_off);
+  G.alist_cap = (c.slab_bytes - kLocalRec - L.alist_off) / 4;
+  G.pc = p;
+  G.nrows = nrows;
+  G.W = W;
+  __syncwarp();
+  gen_solve(c, G, 0, s1, s2);
+  return true;
+}
+
+// Solve a task popped from the pool; the block goes back to the free ring as
+// soon as its contents are in registers or in the slab.
+__device__ void solve_block(const Ctx &c, uint32_t blk) {
+  const EnumParams &P = *c.P;
+  const char *rec = pool_block(P, blk);
+  const uint32_t *hw = (const uint32_t *)rec;
+  const uint32_t pc = ld_cg(hw + 0), nrows = ld_cg(hw + 1), W = ld_cg(hw + 2), rsize = ld_cg(hw + 3);
+  const uint64_t s1 = ld_cg((const uint64_t *)(rec + 16)), s2 = ld_cg((const uint64_t *)(rec + 24));
+  const uint32_t slot = ld_cg(hw + 8);
+  set_slot(c, slot);
+  if (W == 1 && pc <= 32 && nrows <= 32) {
+    T0 t0;
+    t0_load<true>(c, rec, t0, pc, nrows);
+    pool_free(c, blk);
+    t0_solve(c, t0, pc, nrows, rsize, s1, s2);
+    return;
+  }
+  if (W == 1 && nrows <= kT1Rows) {
+    T1 t;
+    t1_load<true>(c, rec, t, pc, nrows);
+    pool_free(c, blk);
+    t1_solve(c, t, pc, nrows, rsize, s1, s2);
+    return;
+  }
+  const Layout L = layout_for(pc, pc, nrows, W);
+  if (L.need > c.slab_bytes) {
+    if (c.lane == 0) atomicExch(P.error, 2u);
+    pool_free(c, blk);
+    return;
+  }
+  uint32_t *colv = (uint32_t *)(c.slab + L.colv_off);
+  const uint32_t *scol = (const uint32_t *)(rec + kHdr);
+  for (uint32_t j = c.lane; j < pc; j += 32) colv[j] = ld_cg(scol + j);
+  uint64_t *rows = (uint64_t *)(c.slab + L.rows_off);
+  const uint64_t *srows = (const uint64_t *)(rec + kHdr + align8(4ULL * pc));
+  const uint64_t nw = (uint64_t)nrows * W;
+  for (uint64_t i = c.lane; i < nw; i += 32) rows[i] = ld_cg(srows + i);
+  uint64_t *h1s = (uint64_t *)(c.slab + L.hash_off);
+  uint64_t *h2s = h1s + pc;
+  __syncwarp();
+  for (uint32_t j = c.lane; j < pc; j += 32) {
+    h1s[j] = P.g.h1[colv[j]];
+    h2s[j] = P.g.h2[colv[j]];
+  }
+  pool_free(c, blk);
+  Gen G;
+  G.rows = rows;
+  G.colv = colv;
+  G.h1s = h1s;
+  G.h2s = h2s;
+  G.stack = (uint64_t *)(c.slab + L.stack_off);
+  G.alist = (uint32_t *)(c.slab + L.alist_off);
+  G.alist_cap = (c.slab_bytes - kLocalRec - L.alist_off) / 4;
+  G.pc = pc;
+  G.nrows = nrows;
+  G.W = W;
+  __syncwarp();
+  gen_solve(c, G, rsize, s1, s2);
+}
+
+__global__ void __launch_bounds__(256, 2) k_enumerate(const __grid_constant__ EnumParams P) {
+  extern __shared__ uint64_t smem_raw[];
+  Ctx c;
+  c.P = &P;
+  c.lane = lane_id();
+  WarpSmem *sm = (WarpSmem *)smem_raw + (threadIdx.x >> 5);
+  c.sm = sm;
+  for (uint32_t b = c.lane; b < kHistCache; b += 32) sm->hcache[b] = 0;
+  if (c.lane == 0) {
+    sm->count = sm->checksum = sm->nodes = sm->wops = 0;
+    sm->max_size = sm->slot = sm->pending = 0;
+    for (int i = 0; i < kCycPhases; i++) sm->cyc[i] = 0;
+  }
   const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  uint64_t *rowbuf = smem + wib * 64;
-  uint32_t *hcache = (uint32_t *)(smem + (blockDim.x >> 5) * 64) + wib * kHistCache;
-  for (uint32_t b = lane; b < kHistCache; b += 32) hcache[b] = 0;
-  WarpAcc acc{0, 0, 0, 0, 0};
-  char *slab = P.slab + gwarp * P.slab_bytes;
+  c.slab = P.slab + gwarp * P.slab_bytes;
+  c.slab_bytes = P.slab_bytes;
+  c.sharing = P.sharing != 0;
   const bool range_mode = P.heavy_list == nullptr && P.root_list == nullptr;
   const uint64_t total = range_mode ? P.re - P.rb : P.n_list;
   unsigned long long nroots = 0;
+  bool roots_left = true;
+  uint64_t idle_spins = 0;
+  // a warp counts itself busy from its first root claim until a claim fails,
+  // so warps that start late (not co-resident) are never waited for
+  if (c.lane == 0) atomicAdd(P.active, 1u);
   __syncwarp();
   for (;;) {
-    unsigned long long k = 0;
-    if (lane == 0) k = atomicAdd(P.next, 1ULL);
-    k = __shfl_sync(kFull, k, 0);
-    if (k >= total) break;
-    uint64_t r;
-    if (P.heavy_list) r = P.heavy_list[k];
-    else if (P.root_list) r = P.root_list[k];
-    else r = P.re - 1 - k;  // heavy (late-peeled) roots first
-    const uint32_t v0 = P.g.root_v0[r], v1 = P.g.root_v1[r];
-    const uint32_t slot = P.g.slot ? P.g.slot[v0] : 0;
-    if (slot != acc.slot) {
-      acc_flush(P, acc, hcache, lane);
-      acc.slot = slot;
-    }
-    const unsigned long long c_before = acc.count, h_before = acc.checksum;
-    nroots++;
-    uint32_t *cand = (uint32_t *)slab;
-    const uint32_t nc = intersect(P.g, v0, v1, cand, P.slab_bytes / 4);
-    bool deferred = false;
-    if (nc == 0xffffffffu) {
-      deferred = true;
-      if (P.push_heavy && lane == 0) {
-        P.heavy_out[atomicAdd(P.heavy_n, 1u)] = (uint32_t)r;
-        uint32_t dmin = min(P.g.off[v0 + 1] - P.g.off[v0], P.g.off[v1 + 1] - P.g.off[v1]);
-        atomicMax(P.heavy_need, (unsigned long long)layout_for(dmin, dmin, dmin, (dmin + 63) / 64).need);
-      } else if (!P.push_heavy && lane == 0) {
-        atomicExch(P.error, 2u);  // does not fit even the large slab
-      }
-    } else {
-      const uint32_t x = nc ? lower_bound_u32(cand, nc, v1) : 0;
-      const uint32_t p = nc - x;
-      const uint64_t s1 = P.g.h1[v0] + P.g.h1[v1], s2 = P.g.h2[v0] + P.g.h2[v1];
-      if (p == 0) {
-        if (x == 0 && lane == 0) emit(P, acc, hcache, 2, s1, s2);
-      } else {
-        const uint32_t W = (p + 63) / 64;
-        const RootLayout L = layout_for(nc, p, x, W);
-        if (L.need > P.slab_bytes) {
-          deferred = true;
-          if (lane == 0) {
-            if (P.push_heavy) {
-              P.heavy_out[atomicAdd(P.heavy_n, 1u)] = (uint32_t)r;
-              atomicMax(P.heavy_need, (unsigned long long)L.need);
-            } else {
-              atomicExch(P.error, 2u);
-            }
-          }
-        } else {
-          uint64_t *h1s = (uint64_t *)(slab + L.hash_off);
-          uint64_t *h2s = h1s + p;
-          uint64_t *rows = (uint64_t *)(slab + L.rows_off);
-          uint64_t *stack = (uint64_t *)(slab + L.stack_off);
-          uint32_t *alist = (uint32_t *)(slab + L.alist_off);
-          const uint64_t alist_cap = (P.slab_bytes - L.alist_off) / 4;
-          for (uint32_t j = lane; j < p; j += 32) {
-            uint32_t y = cand[x + j];
-            h1s[j] = P.g.h1[y];
-            h2s[j] = P.g.h2[y];
-          }
-          const uint32_t nrows = build_rows(P.g, cand, x, p, W, rows, rowbuf);
-          __syncwarp();
-          solve_ego(P, acc, hcache, rows, h1s, h2s, stack, alist, alist_cap, p, nrows, W, s1, s2);
+    if (roots_left) {
+      // queued tasks first: they are the open top of the heaviest subtrees
+      if (c.sharing) {
+        bool got = false;
+        uint32_t b = 0;
+        const unsigned long long tq = now();
+        if (c.lane == 0) got = ring_pop(P.ready_slot, P.ready_seq, P.ready_head, P.ready_tail, P.pool_mask, &b, P);
+        got = __shfl_sync(kFull, got, 0);
+        const uint32_t blk = __shfl_sync(kFull, b, 0);
+        if (c.lane == 0) sm->cyc[kCycQueue] += now() - tq;
+        if (got) {
+          solve_block(c, blk);
+          continue;
         }
       }
+      unsigned long long k = 0;
+      if (c.lane == 0) k = atomicAdd(P.next, 1ULL);
+      k = __shfl_sync(kFull, k, 0);
+      if (k < total) {
+        uint64_t r;
+        if (P.heavy_list) r = P.heavy_list[k];
+        else if (P.root_list) r = P.root_list[k];
+        else r = P.re - 1 - k;  // late-peeled roots first
+        const unsigned long long c0 = sm->count, h0 = sm->checksum;
+        nroots++;
+        const bool fit = solve_root(c, r);
+        if (!fit && c.lane == 0) {
+          if (P.push_heavy) {
+            P.heavy_out[atomicAdd(P.heavy_n, 1u)] = (uint32_t)r;
+            const uint32_t v0 = P.g.root_v0[r], v1 = P.g.root_v1[r];
+            const uint32_t dmin = min(P.g.off[v0 + 1] - P.g.off[v0], P.g.off[v1 + 1] - P.g.off[v1]);
+            atomicMax(P.heavy_need, (unsigned long long)layout_for(dmin, dmin, dmin, (dmin + 63) / 64).need);
+          } else {
+            atomicExch(P.error, 2u);
+          }
+        }
+        if (P.per_root_count && c.lane == 0) {
+          P.per_root_count[k] = fit ? sm->count - c0 : ~0ULL;
+          P.per_root_checksum[k] = sm->checksum - h0;
+        }
+        __syncwarp();
+        continue;
+      }
+      roots_left = false;
+      if (c.lane == 0) atomicSub(P.active, 1u);
+      if (!c.sharing) break;
     }
-    if (lane == 0 && acc.pending > (1u << 30)) acc.pending = kFull;  // force flush below
-    if (__shfl_sync(kFull, acc.pending, 0) == kFull) acc_flush(P, acc, hcache, lane);
-    if (P.per_root_count && lane == 0) {
-      P.per_root_count[k] = deferred ? ~0ULL : acc.count - c_before;
-      P.per_root_checksum[k] = acc.checksum - h_before;
+    // Idle.  Read the busy count before the queue: a task is published before
+    // its producer stops counting as busy, so "nobody busy" followed by "queue
+    // empty" means no work can appear any more.  An idle warp counts itself
+    // busy only when it sees a queued task, and before it takes it.
+    bool done = false, got = false;
+    uint32_t b = 0;
+    const unsigned long long ti0 = now();
+    if (c.lane == 0) {
+      const uint32_t act = *(volatile unsigned int *)P.active;
+      __threadfence();
+      const unsigned long long rh = *(volatile unsigned long long *)P.ready_head;
+      const unsigned long long rt = *(volatile unsigned long long *)P.ready_tail;
+      if (rh < rt) {
+        atomicAdd(P.active, 1u);
+        got = ring_pop(P.ready_slot, P.ready_seq, P.ready_head, P.ready_tail, P.pool_mask, &b, P);
+        if (!got) atomicSub(P.active, 1u);
+      } else if (act == 0) {
+        done = true;
+      } else if (++idle_spins > P.spin_limit) {
+        atomicExch(P.error, 1u);
+        done = true;
+      } else {
+        // back off, with jitter, so idle warps do not hammer the control words
+        const uint32_t shift = idle_spins < 6 ? (uint32_t)idle_spins : 6u;
+        __nanosleep((256u << shift) + ((uint32_t)(clock64() >> 3) & 1023u));
+      }
+      sm->cyc[kCycIdle] += now() - ti0;
     }
-    __syncwarp();
+    got = __shfl_sync(kFull, got, 0);
+    if (got) {
+      solve_block(c, __shfl_sync(kFull, b, 0));
+      if (c.lane == 0) atomicSub(P.active, 1u);
+      idle_spins = 0;
+      continue;
+    }
+    if (__shfl_sync(kFull, done, 0)) break;
   }
-  acc.pending = 0;
-  acc_flush(P, acc, hcache, lane);
-  if (lane == 0) atomicAdd(P.stat_roots, nroots);
+  acc_flush(c);
+  if (c.lane == 0) {
+    atomicAdd(P.stat_roots, nroots);
+    atomicAdd(P.stat_nodes, sm->nodes);
+    atomicAdd(P.stat_wops, sm->wops);
+    for (int i = 0; i < kCycPhases; i++) atomicAdd(P.stat_cycles + i, sm->cyc[i]);
+  }
+}
+
+// Control words; the contended ones each own a 128-byte line.
+struct EnumCtl {
+  alignas(128) unsigned long long next;
+  alignas(128) unsigned long long free_head;
+  alignas(128) unsigned long long free_tail;
+  alignas(128) unsigned long long ready_head;
+  alignas(128) unsigned long long ready_tail;
+  alignas(128) unsigned int active;
+  alignas(128) unsigned long long heavy_need, stat_roots, stat_tasks, stat_nodes, stat_wops;
+  unsigned long long stat_cycles[kCycPhases];
+  unsigned int heavy_n, error;
+};
+
+// free ring full of every block, ready ring empty, counters reset
+__global__ void k_pool_init(EnumCtl *ctl, uint32_t *free_slot, unsigned long long *free_seq,
+                            unsigned long long *ready_seq, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    free_slot[i] = i;
+    free_seq[i] = (unsigned long long)i + 1;  // filled for the consumer of position i
+    ready_seq[i] = i;                        // free for the producer of position i
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    EnumCtl z{};
+    z.free_tail = n;
+    z.active = 0;
+    *ctl = z;
+  }
+}
+
+mce_status reset_ctl(const EnumPlan &plan, cudaStream_t st) {
+  k_pool_init<<<grid_for(plan.pool_blocks, 256), 256, 0, st>>>((EnumCtl *)plan.ctl, plan.params.free_slot,
+                                                               plan.params.free_seq, plan.params.ready_seq,
+                                                               plan.pool_blocks);
+  note_launch();
+  MCE_CUDA_TRY(cudaGetLastError());
+  return MCE_OK;
+}
+
+// Integer-pipe probe: per thread, 8 independent chains of the enumeration's
+// word-op mix (a 64-bit ANDN feeding a 64-bit POPC, folded back by an add).
+__global__ void k_int_probe(const uint64_t *seed, uint64_t *sink, int iters) {
+  uint64_t a[8];
+  const uint64_t b = seed[0] ^ (threadIdx.x * 0x9E3779B97F4A7C15ULL);
+#pragma unroll
+  for (int i = 0; i < 8; i++) a[i] = seed[1] + (uint64_t)i * 0x632BE59BD9B4E019ULL + blockIdx.x;
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) a[i] += __popcll(a[i] & ~b) | (a[i] << 7);
+  }
+  uint64_t x = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) x ^= a[i];
+  if (x == 0x123456789ULL) sink[0] = x;  // keeps the chains live
 }
 
 }  // namespace
-
-struct EnumCtl {
-  unsigned long long next, heavy_need, stat_roots, pad;
-  unsigned int heavy_n, error, pad2[2];
-};
 
 mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, SlotResult *slots,
                      unsigned long long *hist, EnumPlan *plan) {
@@ -530,7 +1657,7 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
   int sms = 0;
   MCE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
   const uint32_t wpb = cfg.warps_per_block ? std::min(cfg.warps_per_block, 8u) : 8u;
-  const uint32_t bps = cfg.blocks_per_sm ? cfg.blocks_per_sm : 2u;
+  const uint32_t bps = cfg.blocks_per_sm ? std::min(cfg.blocks_per_sm, 2u) : 2u;
   EnumParams &P = plan->params;
   P = EnumParams{};
   P.g.n = g.n;
@@ -549,6 +1676,9 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
   P.expand_r = cfg.expand_r;
   P.per_root_count = cfg.per_root_count;
   P.per_root_checksum = cfg.per_root_checksum;
+  P.spin_limit = cfg.spin_limit ? cfg.spin_limit : (1ULL << 34);
+  P.sharing = (cfg.sharing && cfg.per_root_count == nullptr) ? 1 : 0;
+  P.share_bound = cfg.share_bound ? cfg.share_bound : 24;
   mce_status s = MCE_OK;
   EnumCtl *ctl = (EnumCtl *)scr->get(1, sizeof(EnumCtl), &s);
   if (!ctl) return s;
@@ -558,6 +1688,15 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
   P.heavy_n = &ctl->heavy_n;
   P.error = &ctl->error;
   P.stat_roots = &ctl->stat_roots;
+  P.stat_tasks = &ctl->stat_tasks;
+  P.stat_nodes = &ctl->stat_nodes;
+  P.stat_wops = &ctl->stat_wops;
+  P.stat_cycles = ctl->stat_cycles;
+  P.active = &ctl->active;
+  P.free_head = &ctl->free_head;
+  P.free_tail = &ctl->free_tail;
+  P.ready_head = &ctl->ready_head;
+  P.ready_tail = &ctl->ready_tail;
 
   uint64_t rb = cfg.root_begin, re = cfg.root_end ? std::min<uint64_t>(cfg.root_end, g.m) : g.m;
   if (rb > re) rb = re;
@@ -567,29 +1706,49 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
 
   uint32_t blocks = (uint32_t)sms * bps;
   if (cfg.max_blocks && blocks > cfg.max_blocks) blocks = cfg.max_blocks;
-  // never more warps than roots
-  const uint64_t want_blocks = (nwork + wpb - 1) / wpb;
-  if (want_blocks < blocks) blocks = (uint32_t)std::max<uint64_t>(want_blocks, 1);
+  if (!P.sharing) {
+    const uint64_t want_blocks = (nwork + wpb - 1) / wpb;
+    if (want_blocks < blocks) blocks = (uint32_t)std::max<uint64_t>(want_blocks, 1);
+  }
   const uint64_t nwarps = (uint64_t)blocks * wpb;
-  // normal-pass slab: the largest ego network this graph can produce (p <= the
-  // degeneracy, x <= the max degree), capped at 4 MB per warp and by free memory
+  P.nwarps = (uint32_t)nwarps;
+  // slab: the largest ego network this graph can produce (p <= degeneracy,
+  // rows <= max degree), capped at 4 MB per warp and by free memory
   size_t freeb = 0, totalb = 0;
   MCE_CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
   const uint64_t kcap = std::max<uint32_t>(1, std::min(g.degeneracy, g.max_degree));
   const uint64_t dcap = std::max<uint32_t>(1, g.max_degree);
-  const uint64_t wcap = (kcap + 63) / 64;
-  const uint64_t bound = align8(dcap * 4) + 16 * kcap + 8 * (kcap + dcap) * wcap + 8 * (kcap + 2) * (3 * wcap + 4) +
-                         4 * (kcap + dcap) * 4 + 1024;
-  uint64_t slab_bytes = std::min<uint64_t>(align8(bound), 4ULL << 20);
+  const Layout LB = layout_for(dcap, (uint32_t)kcap, (uint32_t)(kcap + dcap), (uint32_t)((kcap + 63) / 64));
+  const uint64_t bound = align8(LB.need + 3ULL * (kcap + dcap) * 4);
+  uint64_t slab_bytes = std::max<uint64_t>(std::min<uint64_t>(bound, 4ULL << 20), 16ULL << 10);
   while (slab_bytes > (64ULL << 10) && slab_bytes * nwarps > freeb / 2) slab_bytes >>= 1;
-  plan->fits_all = slab_bytes >= align8(bound);
+  plan->fits_all = slab_bytes >= bound;
   char *slab = (char *)scr->get(2, slab_bytes * nwarps, &s);
   if (!slab) return s;
+  // deferred roots need a list unless per-root counts are being attributed
+  const bool defer = cfg.per_root_count == nullptr;
   uint32_t *heavy = nullptr;
-  if (!list_mode && nwork) {
+  if (defer && nwork) {
     heavy = (uint32_t *)scr->get(3, nwork * 4, &s);
     if (!heavy) return s;
   }
+  // task pool: one record per block; both rings have one cell per block
+  const uint32_t block_bytes =
+      (uint32_t)std::min<uint64_t>(std::max<uint64_t>(4096, align8(slab_bytes / 4)), 64 << 10);
+  uint32_t nblocks = 1u << 14;
+  while ((uint64_t)nblocks * block_bytes > (freeb / 8) && nblocks > 1024) nblocks >>= 1;
+  char *pool = (char *)scr->get(5, (uint64_t)nblocks * block_bytes, &s);
+  if (!pool) return s;
+  char *rings = (char *)scr->get(6, (uint64_t)nblocks * 24, &s);
+  if (!rings) return s;
+  P.pool = pool;
+  P.block_bytes = block_bytes;
+  P.pool_mask = nblocks - 1;
+  P.free_seq = (unsigned long long *)rings;
+  P.ready_seq = (unsigned long long *)(rings + (uint64_t)nblocks * 8);
+  P.free_slot = (uint32_t *)(rings + (uint64_t)nblocks * 16);
+  P.ready_slot = (uint32_t *)(rings + (uint64_t)nblocks * 20);
+  plan->pool_blocks = nblocks;
   P.slab = slab;
   P.slab_bytes = slab_bytes;
   P.rb = rb;
@@ -597,19 +1756,22 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
   P.root_list = list_mode ? cfg.root_list : nullptr;
   P.n_list = list_mode ? cfg.n_root_list : 0;
   P.heavy_out = heavy;
-  P.push_heavy = list_mode ? 0 : 1;
+  P.push_heavy = defer ? 1 : 0;
   plan->blocks = blocks;
   plan->threads = wpb * 32;
-  plan->smem = (size_t)wpb * 64 * 8 + (size_t)wpb * kHistCache * 4;
+  plan->smem = (size_t)wpb * sizeof(WarpSmem);
   plan->nwarps = nwarps;
   plan->scr = scr;
+  if (plan->smem > 48 * 1024)
+    MCE_CUDA_TRY(cudaFuncSetAttribute(k_enumerate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan->smem));
   return MCE_OK;
 }
 
 mce_status enum_launch(const EnumPlan &plan, cudaStream_t st) {
-  MCE_CUDA_TRY(cudaMemsetAsync(plan.ctl, 0, sizeof(EnumCtl), st));
+  MCE_TRY(reset_ctl(plan, st));
   if (plan.nwork) {
     k_enumerate<<<plan.blocks, plan.threads, plan.smem, st>>>(plan.params);
+    note_launch();
     MCE_CUDA_TRY(cudaGetLastError());
   }
   return MCE_OK;
@@ -623,42 +1785,58 @@ mce_status enum_finish(const EnumPlan &plan, cudaStream_t st, EnumStats *stats) 
   const uint64_t heavy_roots = h.heavy_n;
   uint64_t launches = plan.nwork ? 1 : 0;
   uint64_t roots = h.stat_roots;
+  uint64_t tasks = h.stat_tasks, nodes = h.stat_nodes, wops = h.stat_wops;
+  uint64_t cycles[kCycPhases];
+  for (int i = 0; i < kCycPhases; i++) cycles[i] = h.stat_cycles[i];
+  uint32_t err = h.error;
   if (h.heavy_n && !h.error) {
-    // heavy pass: large slabs, fewer warps
+    // deferred roots: large slabs, and every warp of the pass shares their work
     size_t freeb = 0, totalb = 0;
     MCE_CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
     const uint64_t need = align8(h.heavy_need) + 4096;
-    const uint64_t hw = std::min<uint64_t>({(uint64_t)h.heavy_n, (uint64_t)(freeb * 0.8) / need, plan.nwarps});
+    const uint64_t hw = std::min<uint64_t>((uint64_t)(freeb * 0.7) / need, plan.nwarps);
     if (hw == 0) return MCE_ERR_OUT_OF_MEMORY;
     mce_status s = MCE_OK;
     char *big = (char *)plan.scr->get(4, need * hw, &s);
     if (!big) return s;
-    EnumParams H = plan.params;
-    H.slab = big;
-    H.slab_bytes = need;
-    H.heavy_list = plan.params.heavy_out;
-    H.root_list = nullptr;
-    H.n_list = h.heavy_n;
-    H.push_heavy = 0;
-    MCE_CUDA_TRY(cudaMemsetAsync(&ctl->next, 0, sizeof(unsigned long long), st));
-    MCE_CUDA_TRY(cudaMemsetAsync(&ctl->stat_roots, 0, sizeof(unsigned long long), st));
+    EnumPlan H = plan;
+    H.params.slab = big;
+    H.params.slab_bytes = need;
+    H.params.heavy_list = plan.params.heavy_out;
+    H.params.root_list = nullptr;
+    H.params.n_list = h.heavy_n;
+    H.params.push_heavy = 0;
     const uint32_t wpb = plan.threads / 32;
-    const uint32_t hb = (uint32_t)((hw + wpb - 1) / wpb);
-    k_enumerate<<<hb, plan.threads, plan.smem, st>>>(H);
+    H.blocks = (uint32_t)std::max<uint64_t>(1, hw / wpb);
+    H.nwarps = (uint64_t)H.blocks * wpb;
+    H.params.nwarps = (uint32_t)H.nwarps;
+    MCE_TRY(reset_ctl(H, st));
+    k_enumerate<<<H.blocks, H.threads, H.smem, st>>>(H.params);
+    note_launch();
     launches++;
     MCE_CUDA_TRY(cudaGetLastError());
-    MCE_CUDA_TRY(cudaMemcpyAsync(&h, ctl, sizeof(EnumCtl), cudaMemcpyDeviceToHost, st));
+    EnumCtl h2{};
+    MCE_CUDA_TRY(cudaMemcpyAsync(&h2, ctl, sizeof(EnumCtl), cudaMemcpyDeviceToHost, st));
     MCE_CUDA_TRY(cudaStreamSynchronize(st));
-    roots = roots - heavy_roots + h.stat_roots;
+    roots = roots - heavy_roots + h2.stat_roots;
+    tasks += h2.stat_tasks;
+    nodes += h2.stat_nodes;
+    wops += h2.stat_wops;
+    for (int i = 0; i < kCycPhases; i++) cycles[i] += h2.stat_cycles[i];
+    err = h2.error;
   }
   if (stats) {
     stats->roots = roots;
     stats->heavy_roots = heavy_roots;
-    stats->error = h.error;
+    stats->shared_tasks = tasks;
+    stats->nodes = nodes;
+    stats->word_ops = wops;
+    for (int i = 0; i < kCycPhases; i++) stats->cycles[i] = cycles[i];
+    stats->error = err;
     stats->launches = launches;
   }
-  if (h.error == 2) return MCE_ERR_OUT_OF_MEMORY;
-  if (h.error) return MCE_ERR_TIMEOUT;
+  if (err == 2) return MCE_ERR_OUT_OF_MEMORY;
+  if (err) return MCE_ERR_TIMEOUT;
   return MCE_OK;
 }
 
@@ -680,6 +1858,35 @@ mce_status enumerate(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
   cudaEventDestroy(e1);
   if (stats) stats->ms_enum = ms;
   return s;
+}
+
+mce_status probe_int_peak(int device, double *word_ops_per_s) {
+  MCE_CUDA_TRY(cudaSetDevice(device));
+  int sms = 0;
+  MCE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  uint64_t *buf = nullptr;
+  MCE_CUDA_TRY(cudaMalloc(&buf, 64));
+  MCE_CUDA_TRY(cudaMemset(buf, 0x5a, 64));
+  const int iters = 4096, threads = 256, blocks = sms * 8;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  k_int_probe<<<blocks, threads>>>(buf, buf + 4, 64);
+  note_launch();
+  cudaEventRecord(e0);
+  k_int_probe<<<blocks, threads>>>(buf, buf + 4, iters);
+  note_launch();
+  cudaEventRecord(e1);
+  const cudaError_t e = cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(buf);
+  if (e != cudaSuccess || ms <= 0) return MCE_ERR_CUDA;
+  // two word-ops (ANDN, POPC) per chain step
+  *word_ops_per_s = 2.0 * 8.0 * iters * (double)threads * blocks / (ms * 1e-3);
+  return MCE_OK;
 }
 
 }  // namespace mce

@@ -97,7 +97,8 @@ struct PeelCtl {
   uint32_t tail;       // entries appended to order[]
   uint32_t head;       // next order[] entry to take
   uint32_t processed;  // entries whose neighbours were decremented
-  uint32_t scan_done;  // warps finished with the level scan
+  uint32_t scan_done;  // scan chunks finished
+  uint32_t scan_next;  // next scan chunk to claim
   uint32_t next_n;     // survivors appended to the next remaining list
   uint32_t min_rest;   // smallest degree > k seen among unclaimed vertices
   uint32_t claimed;    // claims at this level
@@ -113,32 +114,44 @@ __device__ __forceinline__ void peel_claim(uint32_t v, uint32_t *state, uint32_t
   }
 }
 
+constexpr uint32_t kPeelChunk = 1024;
+
+// Termination never assumes all warps run at once: the scan is handed out in
+// chunks, and a level is finished when every chunk is scanned and every
+// claimed vertex is processed.
 __global__ void __launch_bounds__(256) k_peel_level(uint32_t k, const uint32_t *rem, uint32_t nrem,
                                                     uint32_t *rem_next, const uint32_t *off,
                                                     const uint32_t *adj, int *deg, uint32_t *state,
-                                                    uint32_t *order, PeelCtl *ctl, uint32_t total_warps,
+                                                    uint32_t *order, PeelCtl *ctl, uint32_t nchunks,
                                                     uint64_t spin_limit) {
   const uint32_t lane = lane_id();
-  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   // 1) scan the remaining vertices: claim degree <= k, keep the rest
   uint32_t local_min = 0xffffffffu;
-  for (uint32_t i = gwarp * 32 + lane; i < nrem; i += total_warps * 32) {
-    uint32_t v = rem[i];
-    if (state[v] != 0) continue;
-    int d = deg[v];
-    if (d <= (int)k) {
-      peel_claim(v, state, order, ctl);
-    } else {
-      rem_next[atomicAdd(&ctl->next_n, 1u)] = v;
-      local_min = min(local_min, (uint32_t)d);
+  for (;;) {
+    uint32_t ch = 0;
+    if (lane == 0) ch = atomicAdd(&ctl->scan_next, 1u);
+    ch = __shfl_sync(kFull, ch, 0);
+    if (ch >= nchunks) break;
+    const uint32_t end = min(nrem, (ch + 1) * kPeelChunk);
+    for (uint32_t i = ch * kPeelChunk + lane; i < end; i += 32) {
+      const uint32_t v = rem[i];
+      if (state[v] != 0) continue;
+      const int d = deg[v];
+      if (d <= (int)k) {
+        peel_claim(v, state, order, ctl);
+      } else {
+        rem_next[atomicAdd(&ctl->next_n, 1u)] = v;
+        local_min = min(local_min, (uint32_t)d);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence();
+      atomicAdd(&ctl->scan_done, 1u);
     }
   }
   local_min = __reduce_min_sync(kFull, local_min);
-  if (lane == 0) {
-    if (local_min != 0xffffffffu) atomicMin(&ctl->min_rest, local_min);
-    __threadfence();
-    atomicAdd(&ctl->scan_done, 1u);
-  }
+  if (lane == 0 && local_min != 0xffffffffu) atomicMin(&ctl->min_rest, local_min);
   // 2) cascade: process claimed vertices through the order[] queue
   volatile PeelCtl *vc = ctl;
   volatile uint32_t *vorder = order;
@@ -168,7 +181,7 @@ __global__ void __launch_bounds__(256) k_peel_level(uint32_t k, const uint32_t *
         have = true;
         break;
       }
-      if (sd == total_warps && done == t) break;  // no claim can arrive any more
+      if (sd == nchunks && done == t) break;  // no claim can arrive any more
       if (++spins > spin_limit) {
         if (lane == 0) atomicExch(&ctl->error, 1u);
         return;
@@ -306,7 +319,7 @@ mce_status peel(uint32_t n, const uint32_t *off, const uint32_t *adj, const uint
   MCE_CUDA_TRY(cudaMemcpyAsync(deg.p, deg0, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
   MCE_CUDA_TRY(cudaMemsetAsync(state.p, 0, n * sizeof(uint32_t), st));
   MCE_CUDA_TRY(cudaMemsetAsync(order, 0xff, n * sizeof(uint32_t), st));
-  k_iota<<<grid_for(n, 256), 256, 0, st>>>(remA.p, n);
+  k_iota<<<grid_for(n, 256), 256, 0, st>>>(remA.p, n); note_launch();
   int dev = 0;
   MCE_CUDA_TRY(cudaGetDevice(&dev));
   int sms = 0, per_sm = 0;
@@ -314,7 +327,6 @@ mce_status peel(uint32_t n, const uint32_t *off, const uint32_t *adj, const uint
   MCE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel_level, 256, 0));
   // every block must be resident: waiting warps spin on work other warps produce
   uint32_t blocks = (uint32_t)std::max(1, std::min(per_sm, 4)) * (uint32_t)sms;
-  uint32_t total_warps = blocks * 8;
   PeelCtl h{};
   uint32_t nrem = n, tail = 0, k = 0, degen = 0;
   PeelCtl *hc = nullptr;
@@ -331,8 +343,9 @@ mce_status peel(uint32_t n, const uint32_t *off, const uint32_t *adj, const uint
       s = MCE_ERR_CUDA;
       break;
     }
+    const uint32_t nchunks = (nrem + kPeelChunk - 1) / kPeelChunk;
     k_peel_level<<<blocks, 256, 0, st>>>(k, remA.p, nrem, remB.p, off, adj, deg.p, state.p, order, ctl.p,
-                                          total_warps, spin_limit);
+                                          nchunks, spin_limit); note_launch();
     if (cudaGetLastError() != cudaSuccess) {
       s = MCE_ERR_CUDA;
       break;
@@ -366,6 +379,116 @@ mce_status peel(uint32_t n, const uint32_t *off, const uint32_t *adj, const uint
 
 }  // namespace
 
+namespace {
+
+__global__ void k_pack_keys64(const uint32_t *u, const uint32_t *v, uint64_t n, uint64_t *keys) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t a = u[i], b = v[i];
+    if (a == b) {
+      keys[i] = kInvalidKey;  // (a < b) keys never reach all-ones
+      continue;
+    }
+    if (a > b) {
+      uint32_t t = a;
+      a = b;
+      b = t;
+    }
+    keys[i] = ((uint64_t)a << 32) | b;
+  }
+}
+
+__global__ void k_endpoints(const uint64_t *edges, uint64_t m, uint64_t *ends) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+    ends[2 * i] = edges[i] >> 32;
+    ends[2 * i + 1] = edges[i] & 0xffffffffULL;
+  }
+}
+
+__global__ void k_labels_from_sorted(const uint64_t *ends, const uint32_t *flag, const uint32_t *pos, uint64_t k,
+                                     uint32_t *labels) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < k; i += (uint64_t)gridDim.x * blockDim.x)
+    if (flag[i]) labels[pos[i]] = (uint32_t)ends[i];
+}
+
+__device__ __forceinline__ uint32_t find_label(const uint32_t *labels, uint32_t n, uint32_t l) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (labels[mid] < l) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void k_map_edges_search(const uint64_t *edges, uint64_t m, const uint32_t *labels, uint32_t n,
+                                   uint32_t *eu, uint32_t *ev, uint32_t *deg) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t a = find_label(labels, n, (uint32_t)(edges[i] >> 32));
+    const uint32_t b = find_label(labels, n, (uint32_t)(edges[i] & 0xffffffffULL));
+    eu[i] = a;
+    ev[i] = b;
+    atomicAdd(&deg[a], 1u);
+    atomicAdd(&deg[b], 1u);
+  }
+}
+
+// present labels, ascending, by sorting the 2m endpoints; ids by binary search
+mce_status build_sparse_labels(const uint32_t *u, const uint32_t *v, uint64_t np, int order_kind,
+                               uint64_t spin_limit, cudaStream_t st, DeviceGraph *g) {
+  if (np >= (1ULL << 32)) return MCE_ERR_TOO_LARGE;
+  DevBuf<uint64_t> keys, tmp;
+  MCE_TRY(keys.alloc(np, st));
+  MCE_TRY(tmp.alloc(np, st));
+  k_pack_keys64<<<grid_for(np, 256), 256, 0, st>>>(u, v, np, keys.p); note_launch();
+  MCE_TRY(radix_sort_u64(keys.p, tmp.p, np, 64, st));
+  DevBuf<uint32_t> flags, pos;
+  MCE_TRY(flags.alloc(np + 1, st));
+  MCE_TRY(pos.alloc(np + 1, st));
+  k_unique_flags<<<grid_for(np, 256), 256, 0, st>>>(keys.p, np, flags.p); note_launch();
+  MCE_TRY(scan_exclusive_u32(flags.p, pos.p, np, pos.p + np, st));
+  uint32_t m32 = 0;
+  MCE_TRY(read_scalar(pos.p + np, &m32, st));
+  const uint64_t m = m32;
+  if (2 * m >= (1ULL << 32)) return MCE_ERR_TOO_LARGE;
+  DevBuf<uint64_t> edges;
+  MCE_TRY(edges.alloc(m, st));
+  k_compact_keys<<<grid_for(np, 256), 256, 0, st>>>(keys.p, flags.p, pos.p, np, edges.p); note_launch();
+  keys.release();
+  tmp.release();
+  flags.release();
+  pos.release();
+  const uint64_t k = 2 * m;
+  DevBuf<uint64_t> ends, etmp;
+  MCE_TRY(ends.alloc(k, st));
+  MCE_TRY(etmp.alloc(k, st));
+  k_endpoints<<<grid_for(m, 256), 256, 0, st>>>(edges.p, m, ends.p); note_launch();
+  MCE_TRY(radix_sort_u64(ends.p, etmp.p, k, 32, st));
+  etmp.release();
+  DevBuf<uint32_t> f2, p2;
+  MCE_TRY(f2.alloc(k + 1, st));
+  MCE_TRY(p2.alloc(k + 1, st));
+  k_unique_flags<<<grid_for(k, 256), 256, 0, st>>>(ends.p, k, f2.p); note_launch();
+  MCE_TRY(scan_exclusive_u32(f2.p, p2.p, k, p2.p + k, st));
+  uint32_t n = 0;
+  MCE_TRY(read_scalar(p2.p + k, &n, st));
+  DevBuf<uint32_t> labels0, eu, ev, deg;
+  MCE_TRY(labels0.alloc(n, st));
+  MCE_TRY(eu.alloc(m, st));
+  MCE_TRY(ev.alloc(m, st));
+  MCE_TRY(deg.alloc(n + 1, st));
+  k_labels_from_sorted<<<grid_for(k, 256), 256, 0, st>>>(ends.p, f2.p, p2.p, k, labels0.p); note_launch();
+  MCE_CUDA_TRY(cudaMemsetAsync(deg.p, 0, (n + 1) * sizeof(uint32_t), st));
+  k_map_edges_search<<<grid_for(m, 256), 256, 0, st>>>(edges.p, m, labels0.p, n, eu.p, ev.p, deg.p); note_launch();
+  ends.release();
+  f2.release();
+  p2.release();
+  edges.release();
+  MCE_TRY(finish_graph(n, m, eu.p, ev.p, deg.p, labels0.p, order_kind, spin_limit, st, g));
+  return MCE_OK;
+}
+
+}  // namespace
+
 mce_status build_from_pairs(const uint32_t *u, const uint32_t *v, uint64_t np, int order_kind,
                             uint64_t spin_limit, cudaStream_t st, DeviceGraph *g) {
   *g = DeviceGraph{};
@@ -377,6 +500,9 @@ mce_status build_from_pairs(const uint32_t *u, const uint32_t *v, uint64_t np, i
   MCE_CUDA_TRY(cudaMemcpyAsync(hm, maxbuf.p, sizeof(hm), cudaMemcpyDeviceToHost, st));
   MCE_CUDA_TRY(cudaStreamSynchronize(st));
   const uint32_t maxlab = std::max(hm[0], hm[1]);
+  // labels much sparser than the pair count (or near 2^32): sort-based relabel
+  if (maxlab >= (1u << 30) || (uint64_t)maxlab > 8 * np + (1u << 20))
+    return build_sparse_labels(u, v, np, order_kind, spin_limit, st, g);
   const int lb = bits_for(maxlab);
   if (2 * lb > 63) return MCE_ERR_TOO_LARGE;
 
@@ -384,12 +510,12 @@ mce_status build_from_pairs(const uint32_t *u, const uint32_t *v, uint64_t np, i
   DevBuf<uint64_t> keys, tmp;
   MCE_TRY(keys.alloc(np, st));
   MCE_TRY(tmp.alloc(np, st));
-  k_pack_keys<<<grid_for(np, 256), 256, 0, st>>>(u, v, np, lb, keys.p);
+  k_pack_keys<<<grid_for(np, 256), 256, 0, st>>>(u, v, np, lb, keys.p); note_launch();
   MCE_TRY(radix_sort_u64(keys.p, tmp.p, np, 2 * lb, st));
   DevBuf<uint32_t> flags, pos;
   MCE_TRY(flags.alloc(np + 1, st));
   MCE_TRY(pos.alloc(np + 1, st));
-  k_unique_flags<<<grid_for(np, 256), 256, 0, st>>>(keys.p, np, flags.p);
+  k_unique_flags<<<grid_for(np, 256), 256, 0, st>>>(keys.p, np, flags.p); note_launch();
   MCE_TRY(scan_exclusive_u32(flags.p, pos.p, np, pos.p + np, st));
   uint32_t m32 = 0;
   MCE_TRY(read_scalar(pos.p + np, &m32, st));
@@ -397,7 +523,7 @@ mce_status build_from_pairs(const uint32_t *u, const uint32_t *v, uint64_t np, i
   if (np > 0xffffffffULL || 2 * m >= (1ULL << 32)) return MCE_ERR_TOO_LARGE;
   DevBuf<uint64_t> edges;
   MCE_TRY(edges.alloc(m, st));
-  k_compact_keys<<<grid_for(np, 256), 256, 0, st>>>(keys.p, flags.p, pos.p, np, edges.p);
+  k_compact_keys<<<grid_for(np, 256), 256, 0, st>>>(keys.p, flags.p, pos.p, np, edges.p); note_launch();
   keys.release();
   tmp.release();
   flags.release();
@@ -409,7 +535,7 @@ mce_status build_from_pairs(const uint32_t *u, const uint32_t *v, uint64_t np, i
   MCE_TRY(mark.alloc(nl + 1, st));
   MCE_TRY(id.alloc(nl + 1, st));
   MCE_CUDA_TRY(cudaMemsetAsync(mark.p, 0, nl * sizeof(uint32_t), st));
-  k_mark_labels<<<grid_for(m, 256), 256, 0, st>>>(edges.p, m, lb, mark.p);
+  k_mark_labels<<<grid_for(m, 256), 256, 0, st>>>(edges.p, m, lb, mark.p); note_launch();
   MCE_TRY(scan_exclusive_u32(mark.p, id.p, nl, id.p + nl, st));
   uint32_t n = 0;
   MCE_TRY(read_scalar(id.p + nl, &n, st));
@@ -418,9 +544,9 @@ mce_status build_from_pairs(const uint32_t *u, const uint32_t *v, uint64_t np, i
   MCE_TRY(eu.alloc(m, st));
   MCE_TRY(ev.alloc(m, st));
   MCE_TRY(deg.alloc(n + 1, st));
-  k_labels_from_marks<<<grid_for(nl, 256), 256, 0, st>>>(mark.p, id.p, nl, labels0.p);
+  k_labels_from_marks<<<grid_for(nl, 256), 256, 0, st>>>(mark.p, id.p, nl, labels0.p); note_launch();
   MCE_CUDA_TRY(cudaMemsetAsync(deg.p, 0, (n + 1) * sizeof(uint32_t), st));
-  k_map_edges<<<grid_for(m, 256), 256, 0, st>>>(edges.p, m, lb, id.p, eu.p, ev.p, deg.p);
+  k_map_edges<<<grid_for(m, 256), 256, 0, st>>>(edges.p, m, lb, id.p, eu.p, ev.p, deg.p); note_launch();
   mark.release();
   id.release();
   edges.release();
@@ -455,19 +581,19 @@ mce_status finish_graph(uint32_t n, uint64_t m, const uint32_t *eu, const uint32
     MCE_TRY(adj0.alloc(2 * m, st));
     MCE_TRY(scan_exclusive_u32(deg, off0.p, n, off0.p + n, st));
     MCE_CUDA_TRY(cudaMemcpyAsync(cursor.p, off0.p, (n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-    k_fill_adj<<<grid_for(m, 256), 256, 0, st>>>(eu, ev, m, cursor.p, adj0.p);
+    k_fill_adj<<<grid_for(m, 256), 256, 0, st>>>(eu, ev, m, cursor.p, adj0.p); note_launch();
     MCE_TRY(peel(n, off0.p, adj0.p, deg, order.p, &g->degeneracy, spin_limit, st));
   } else if ((order_kind == MCE_ORDER_DEGREE_ASC || order_kind == MCE_ORDER_DEGREE_DESC) && n > 0) {
     DevBuf<uint64_t> dk, dt;
     MCE_TRY(dk.alloc(n, st));
     MCE_TRY(dt.alloc(n, st));
-    k_degree_keys<<<grid_for(n, 256), 256, 0, st>>>(deg, n, order_kind == MCE_ORDER_DEGREE_DESC, dk.p);
+    k_degree_keys<<<grid_for(n, 256), 256, 0, st>>>(deg, n, order_kind == MCE_ORDER_DEGREE_DESC, dk.p); note_launch();
     MCE_TRY(radix_sort_u64(dk.p, dt.p, n, 64, st));
-    k_order_from_keys<<<grid_for(n, 256), 256, 0, st>>>(dk.p, n, order.p);
+    k_order_from_keys<<<grid_for(n, 256), 256, 0, st>>>(dk.p, n, order.p); note_launch();
   } else {
-    k_iota<<<grid_for(n, 256), 256, 0, st>>>(order.p, n);
+    k_iota<<<grid_for(n, 256), 256, 0, st>>>(order.p, n); note_launch();
   }
-  k_rank_from_order<<<grid_for(n, 256), 256, 0, st>>>(order.p, n, rank.p);
+  k_rank_from_order<<<grid_for(n, 256), 256, 0, st>>>(order.p, n, rank.p); note_launch();
   order.release();
 
   // 4) relabelled symmetric edge keys -> sorted CSR
@@ -479,7 +605,7 @@ mce_status finish_graph(uint32_t n, uint64_t m, const uint32_t *eu, const uint32
   DevBuf<uint32_t> deg_new;
   MCE_TRY(deg_new.alloc(n + 1, st));
   MCE_CUDA_TRY(cudaMemsetAsync(deg_new.p, 0, (n + 1) * sizeof(uint32_t), st));
-  k_relabel_keys<<<grid_for(m, 256), 256, 0, st>>>(eu, ev, m, rank.p, nb, keys.p, deg_new.p);
+  k_relabel_keys<<<grid_for(m, 256), 256, 0, st>>>(eu, ev, m, rank.p, nb, keys.p, deg_new.p); note_launch();
   MCE_TRY(radix_sort_u64(keys.p, tmp.p, m2, 2 * nb, st));
   tmp.release();
   MCE_CUDA_TRY(cudaMallocAsync(&g->off, (n + 1) * sizeof(uint32_t), st));
@@ -488,18 +614,18 @@ mce_status finish_graph(uint32_t n, uint64_t m, const uint32_t *eu, const uint32
   DevBuf<uint32_t> upflag, uppos;
   MCE_TRY(upflag.alloc(m2 + 1, st));
   MCE_TRY(uppos.alloc(m2 + 1, st));
-  k_csr_cols<<<grid_for(m2, 256), 256, 0, st>>>(keys.p, m2, nb, g->adj, upflag.p);
+  k_csr_cols<<<grid_for(m2, 256), 256, 0, st>>>(keys.p, m2, nb, g->adj, upflag.p); note_launch();
   MCE_TRY(scan_exclusive_u32(upflag.p, uppos.p, m2, uppos.p + m2, st));
   MCE_CUDA_TRY(cudaMallocAsync(&g->root_v0, std::max<uint64_t>(m, 1) * sizeof(uint32_t), st));
   MCE_CUDA_TRY(cudaMallocAsync(&g->root_v1, std::max<uint64_t>(m, 1) * sizeof(uint32_t), st));
-  k_roots<<<grid_for(m2, 256), 256, 0, st>>>(keys.p, m2, nb, upflag.p, uppos.p, g->root_v0, g->root_v1);
+  k_roots<<<grid_for(m2, 256), 256, 0, st>>>(keys.p, m2, nb, upflag.p, uppos.p, g->root_v0, g->root_v1); note_launch();
   keys.release();
 
   // 5) labels and their hashes under the new ids
   MCE_CUDA_TRY(cudaMallocAsync(&g->labels, std::max<uint32_t>(n, 1) * sizeof(uint32_t), st));
   MCE_CUDA_TRY(cudaMallocAsync(&g->h1, std::max<uint32_t>(n, 1) * sizeof(uint64_t), st));
   MCE_CUDA_TRY(cudaMallocAsync(&g->h2, std::max<uint32_t>(n, 1) * sizeof(uint64_t), st));
-  k_permute_labels<<<grid_for(n, 256), 256, 0, st>>>(labels0, rank.p, n, g->labels, g->h1, g->h2);
+  k_permute_labels<<<grid_for(n, 256), 256, 0, st>>>(labels0, rank.p, n, g->labels, g->h1, g->h2); note_launch();
   MCE_CUDA_TRY(cudaGetLastError());
   MCE_CUDA_TRY(cudaStreamSynchronize(st));
   return MCE_OK;
@@ -521,7 +647,7 @@ mce_status build_from_csr(uint64_t n, const uint32_t *off_d, const uint32_t *adj
   if (labels_d)
     MCE_CUDA_TRY(cudaMemcpyAsync(labels0.p, labels_d, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
   else
-    k_iota<<<grid_for(n, 256), 256, 0, st>>>(labels0.p, n);
+    k_iota<<<grid_for(n, 256), 256, 0, st>>>(labels0.p, n); note_launch();
   MCE_TRY(csr_to_edges(n, off_d, adj_d, m, deg.p, &eu.p, &ev.p, st));
   eu.st = ev.st = st;
   MCE_TRY(finish_graph((uint32_t)n, m, eu.p, ev.p, deg.p, labels0.p,
@@ -557,18 +683,18 @@ __global__ void k_upper_edges(const uint32_t *off, const uint32_t *adj, uint64_t
 
 mce_status csr_to_edges(uint64_t n, const uint32_t *off, const uint32_t *adj, uint64_t m, uint32_t *deg,
                         uint32_t **eu, uint32_t **ev, cudaStream_t st) {
-  k_degrees_from_off<<<grid_for(n, 256), 256, 0, st>>>(off, n, deg);
+  k_degrees_from_off<<<grid_for(n, 256), 256, 0, st>>>(off, n, deg); note_launch();
   DevBuf<uint32_t> flag, pos;
   MCE_TRY(flag.alloc(2 * m + 1, st));
   MCE_TRY(pos.alloc(2 * m + 1, st));
-  k_upper_flags<<<grid_for(n * 32, 256), 256, 0, st>>>(off, adj, n, flag.p);
+  k_upper_flags<<<grid_for(n * 32, 256), 256, 0, st>>>(off, adj, n, flag.p); note_launch();
   MCE_TRY(scan_exclusive_u32(flag.p, pos.p, 2 * m, pos.p + 2 * m, st));
   uint32_t mu = 0;
   MCE_TRY(read_scalar(pos.p + 2 * m, &mu, st));
   if (mu != m) return MCE_ERR_FORMAT;  // not symmetric / has self-loops
   MCE_CUDA_TRY(cudaMallocAsync(eu, std::max<uint64_t>(m, 1) * sizeof(uint32_t), st));
   MCE_CUDA_TRY(cudaMallocAsync(ev, std::max<uint64_t>(m, 1) * sizeof(uint32_t), st));
-  k_upper_edges<<<grid_for(n * 32, 256), 256, 0, st>>>(off, adj, n, flag.p, pos.p, *eu, *ev);
+  k_upper_edges<<<grid_for(n * 32, 256), 256, 0, st>>>(off, adj, n, flag.p, pos.p, *eu, *ev); note_launch();
   MCE_CUDA_TRY(cudaGetLastError());
   return MCE_OK;
 }

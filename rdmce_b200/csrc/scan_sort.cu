@@ -8,6 +8,7 @@
 // that ranks keys with __match_any_sync, reorders the tile in shared memory and
 // writes runs of equal digits contiguously.
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -111,16 +112,16 @@ mce_status scan_impl(const T *in, T *out, uint64_t n, T *d_total, cudaStream_t s
   }
   uint64_t tiles = (n + kScanTile - 1) / kScanTile;
   if (tiles == 1) {
-    k_tile_scan<T><<<1, kScanThreads, 0, st>>>(in, out, n, nullptr, d_total);
+    k_tile_scan<T><<<1, kScanThreads, 0, st>>>(in, out, n, nullptr, d_total); note_launch();
     MCE_CUDA_TRY(cudaGetLastError());
     return MCE_OK;
   }
   T *sums = nullptr;
   MCE_CUDA_TRY(cudaMallocAsync(&sums, tiles * sizeof(T), st));
-  k_tile_sums<T><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, n, sums);
+  k_tile_sums<T><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, n, sums); note_launch();
   mce_status s = scan_impl<T>(sums, sums, tiles, (T *)nullptr, st);
   if (s == MCE_OK) {
-    k_tile_scan<T><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, n, sums, d_total);
+    k_tile_scan<T><<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, n, sums, d_total); note_launch();
     if (cudaGetLastError() != cudaSuccess) s = MCE_ERR_CUDA;
   }
   cudaFreeAsync(sums, st);
@@ -220,6 +221,7 @@ __global__ void k_reduce_max(const uint32_t *in, uint64_t n, uint32_t *out) {
   if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
 }
 
+std::atomic<uint64_t> g_launches{0};
 std::mutex g_default_mu[64];
 Scratch g_default[64];
 
@@ -243,10 +245,10 @@ mce_status radix_sort_u64(uint64_t *keys, uint64_t *tmp, uint64_t n, int bits, c
   uint64_t *src = keys, *dst = tmp;
   mce_status s = MCE_OK;
   for (int shift = 0; shift < bits && s == MCE_OK; shift += 8) {
-    k_radix_hist<<<ntiles, kSortThreads, 0, st>>>(src, n, shift, hist, ntiles);
+    k_radix_hist<<<ntiles, kSortThreads, 0, st>>>(src, n, shift, hist, ntiles); note_launch();
     s = scan_exclusive_u32(hist, hist, (uint64_t)ntiles * kRadix, nullptr, st);
     if (s != MCE_OK) break;
-    k_radix_scatter<<<ntiles, kSortThreads, 0, st>>>(src, dst, n, shift, hist, ntiles);
+    k_radix_scatter<<<ntiles, kSortThreads, 0, st>>>(src, dst, n, shift, hist, ntiles); note_launch();
     if (cudaGetLastError() != cudaSuccess) s = MCE_ERR_CUDA;
     uint64_t *t = src;
     src = dst;
@@ -263,7 +265,7 @@ mce_status radix_sort_u64(uint64_t *keys, uint64_t *tmp, uint64_t n, int bits, c
 mce_status reduce_max_u32(const uint32_t *in, uint64_t n, uint32_t *d_out, cudaStream_t st) {
   MCE_CUDA_TRY(cudaMemsetAsync(d_out, 0, sizeof(uint32_t), st));
   if (n == 0) return MCE_OK;
-  k_reduce_max<<<grid_for(n, 256, 148 * 8), 256, 0, st>>>(in, n, d_out);
+  k_reduce_max<<<grid_for(n, 256, 148 * 8), 256, 0, st>>>(in, n, d_out); note_launch();
   MCE_CUDA_TRY(cudaGetLastError());
   return MCE_OK;
 }
@@ -296,6 +298,8 @@ void Scratch::release() {
   }
 }
 
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
 Scratch *default_scratch(int device) {
   Scratch *s = &g_default[device & 63];
   s->device = device;
@@ -305,3 +309,5 @@ void lock_default(int device) { g_default_mu[device & 63].lock(); }
 void unlock_default(int device) { g_default_mu[device & 63].unlock(); }
 
 }  // namespace mce
+
+extern "C" uint64_t mce_launch_count(void) { return mce::g_launches.load(); }
