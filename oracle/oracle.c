@@ -35,6 +35,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #define GOLDEN 0x9E3779B97F4A7C15ULL
 
@@ -389,6 +390,7 @@ typedef struct {
   uint32_t v0, v1;
   FILE *out;
   og_result *res;
+  atomic_int *stop; /* og_mce_roots_timed: set at the deadline, unwinds the search */
 } bk_ctx;
 
 static void *grow(void *p, size_t *cap, size_t need, size_t elem) {
@@ -430,6 +432,7 @@ static void emit(bk_ctx *c, uint32_t size, uint64_t s1, uint64_t s2, const uint6
 static void bk_node(bk_ctx *c, size_t po, size_t ao, uint32_t nA, uint32_t rsize, uint64_t s1, uint64_t s2) {
   const uint32_t W = c->W;
   og_result *res = c->res;
+  if (c->stop && atomic_load_explicit(c->stop, memory_order_relaxed)) return;
   res->nodes++;
   {
     const uint64_t *P = c->pbuf + po;
@@ -593,6 +596,9 @@ typedef struct {
   atomic_uint_fast64_t next;
   og_result *partial;
   int nthreads;
+  atomic_int stop;
+  atomic_int running;
+  int timed;
 } job_t;
 
 typedef struct { job_t *job; int tid; } targ_t;
@@ -605,9 +611,11 @@ static void *worker(void *arg) {
   c.g = J->g;
   c.expand_r = J->expand_r;
   c.res = &J->partial[t->tid];
-  const uint64_t chunk = 16;
+  if (J->timed) c.stop = &J->stop;
+  const uint64_t chunk = J->timed ? 1 : 16;
   uint64_t total = J->end - J->begin;
   for (;;) {
+    if (J->timed && atomic_load(&J->stop)) break;
     uint64_t k0 = atomic_fetch_add(&J->next, chunk);
     if (k0 >= total) break;
     uint64_t k1 = k0 + chunk < total ? k0 + chunk : total;
@@ -626,24 +634,46 @@ static void *worker(void *arg) {
     }
   }
   ctx_free(&c);
+  atomic_fetch_sub(&J->running, 1);
   return NULL;
 }
 
-static int run_job(job_t *J, int threads) {
+static double now_s(void) {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+/* seconds > 0: stop the search at the deadline (partial counts are kept) */
+static int run_job_until(job_t *J, int threads, double seconds, double *elapsed) {
   if (threads < 1) threads = 1;
   J->nthreads = threads;
   J->partial = (og_result *)calloc((size_t)threads, sizeof(og_result));
   atomic_init(&J->next, 0);
+  atomic_init(&J->stop, 0);
+  atomic_init(&J->running, threads);
+  J->timed = seconds > 0;
   pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * (size_t)threads);
   targ_t *ta = (targ_t *)malloc(sizeof(targ_t) * (size_t)threads);
+  const double t0 = now_s();
   for (int i = 0; i < threads; i++) {
     ta[i].job = J; ta[i].tid = i;
     pthread_create(&th[i], NULL, worker, &ta[i]);
   }
+  if (J->timed) {
+    while (atomic_load(&J->running) > 0 && now_s() - t0 < seconds) {
+      struct timespec ts = {0, 5 * 1000 * 1000};
+      nanosleep(&ts, NULL);
+    }
+    atomic_store(&J->stop, 1);
+  }
   for (int i = 0; i < threads; i++) pthread_join(th[i], NULL);
+  if (elapsed) *elapsed = now_s() - t0;
   free(th); free(ta);
   return 0;
 }
+
+static int run_job(job_t *J, int threads) { return run_job_until(J, threads, 0.0, NULL); }
 
 static void merge(og_result *out, const og_result *in, int k) {
   memset(out, 0, sizeof(*out));
@@ -683,6 +713,24 @@ int og_mce_roots(const og_graph *g, const uint64_t *roots, uint64_t nroots, int 
   J.expand_r = 1;
   run_job(&J, threads);
   free(J.partial);
+  return 0;
+}
+
+int og_mce_roots_timed(const og_graph *g, const uint64_t *roots, uint64_t nroots, int threads, double seconds,
+                       og_result *out, uint64_t *roots_started, double *elapsed) {
+  build_root_off((og_graph *)g);
+  for (uint64_t k = 0; k < nroots; k++)
+    if (roots[k] >= g->m) return -1;
+  uint64_t *cnt = (uint64_t *)calloc(nroots ? nroots : 1, 8), *chk = (uint64_t *)calloc(nroots ? nroots : 1, 8);
+  job_t J;
+  memset(&J, 0, sizeof(J));
+  J.g = g; J.begin = 0; J.end = nroots; J.roots = roots; J.counts = cnt; J.checksums = chk;
+  J.expand_r = 1;
+  run_job_until(&J, threads, seconds, elapsed);
+  merge(out, J.partial, J.nthreads);
+  uint64_t started = atomic_load(&J.next);
+  if (roots_started) *roots_started = started < nroots ? started : nroots;
+  free(J.partial); free(cnt); free(chk);
   return 0;
 }
 

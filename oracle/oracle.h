@@ -72,6 +72,12 @@ int og_mce(const og_graph *g, uint64_t begin, uint64_t end, int threads, int exp
 int og_mce_roots(const og_graph *g, const uint64_t *roots, uint64_t nroots, int threads,
                  uint64_t *counts, uint64_t *checksums);
 /* Write every maximal clique (original labels, ascending) as lines into a file. */
+/* Time-bounded variant for CPU baselines: threads claim roots of the list
+ * until `seconds` pass, then the search unwinds; `out` holds what was found
+ * by then (count, histogram, nodes), `roots_started` the roots claimed. */
+int og_mce_roots_timed(const og_graph *g, const uint64_t *roots, uint64_t nroots, int threads, double seconds,
+                       og_result *out, uint64_t *roots_started, double *elapsed);
+
 int og_list_cliques(const og_graph *g, const char *path);
 
 /* Per-root ego sizes p, x (all common neighbours below v1) and x after X-row compaction. */

@@ -80,6 +80,8 @@ def lib():
             "og_root": (None, [P, U64, C.POINTER(U32), C.POINTER(U32)]),
             "og_mce": (I, [P, U64, U64, I, I, C.POINTER(_Result)]),
             "og_mce_roots": (I, [P, P, U64, I, P, P]),
+            "og_mce_roots_timed": (I, [P, P, U64, I, C.c_double, C.POINTER(_Result), C.POINTER(U64),
+                                       C.POINTER(C.c_double)]),
             "og_list_cliques": (I, [P, C.c_char_p]),
             "og_store_bin": (I, [P, C.c_char_p]),
             "og_load_bin": (P, [C.c_char_p]),
@@ -203,6 +205,19 @@ class Graph:
         if lib().og_mce_roots(self.h, _ptr(roots), len(roots), threads, _ptr(cnt), _ptr(chk)) != 0:
             raise ValueError("root id out of range")
         return cnt, chk
+
+    def mce_roots_timed(self, roots, threads, seconds):
+        """Cliques found under the listed roots within `seconds` (all threads);
+        returns (OracleResult so far, roots started, elapsed seconds)."""
+        roots = np.ascontiguousarray(roots, dtype=np.uint64)
+        res = _Result()
+        started, el = C.c_uint64(), C.c_double()
+        if lib().og_mce_roots_timed(self.h, _ptr(roots), len(roots), threads, seconds, C.byref(res),
+                                    C.byref(started), C.byref(el)) != 0:
+            raise ValueError("root id out of range")
+        hist = {s: int(res.hist[s]) for s in range(HIST_LEN) if res.hist[s]}
+        return (OracleResult(res.count, res.checksum, hist, res.max_size, res.nodes, res.pivot_words,
+                             res.filter_rows, res.build_bytes), started.value, el.value)
 
     def list_cliques(self, path):
         if lib().og_list_cliques(self.h, path.encode()) != 0:

@@ -1,0 +1,211 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle and the
+golden fixtures.  Integer results are compared bit-exactly: clique count,
+clique-size histogram, order-independent checksum, largest clique, degeneracy.
+
+Coverage follows the reference's own checks (RDMCE scripts/analyze.sh compares
+the "MC numbers" line across configurations; main.cc `-o` orders): every vertex
+order, task sharing on and off, EXPAND_R on and off, root ranges and root lists,
+every enumeration tier boundary, and the loader's edge cases.
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import edges_uv, golden_fixtures, opts
+
+pytestmark = pytest.mark.gpu
+
+THREADS = max(1, min(32, os.cpu_count() or 1))
+
+
+def assert_same(r, o, what=""):
+    assert r.count == o.count, what
+    assert r.checksum == o.checksum, what
+    assert r.hist == o.hist, what
+    assert r.max_size == o.max_size, what
+
+
+def oracle_result(oracle_mod, u, v, threads=THREADS):
+    g = oracle_mod.Graph.from_pairs(u, v).sort_degeneracy()
+    return g, g.mce(threads=threads)
+
+
+@pytest.mark.parametrize("fx", golden_fixtures(), ids=lambda f: f["name"])
+def test_golden(gpu, fx):
+    u, v = edges_uv(fx)
+    o = opts(gpu)
+    with gpu.Graph.from_coo(u, v, o) as g:
+        info = g.info()
+        assert (info["num_vertices"], info["num_edges"], info["degeneracy"]) == (fx["n"], fx["m"], fx["degeneracy"])
+        r = g.solve(o)
+    assert r.count == fx["count"]
+    assert f"{r.checksum:016x}" == fx["checksum"]
+    assert {str(k): c for k, c in r.hist.items()} == fx["hist"]
+
+
+def _cases(engine):
+    yield "chung_lu_1e4", engine.gen_chung_lu(10000, 16, 2.5, 1)
+    yield "rmat12", engine.gen_rmat(12, 16, 3)
+    yield "rmat13_ef8", engine.gen_rmat(13, 8, 4)
+    for s in range(3):
+        yield f"gnp400_{s}", engine.gen_gnp(400, 40, 200 + s)
+    u, v = engine.gen_planted(2000, 3, 100, 200, 9)
+    u2, v2 = engine.gen_gnp(2000, 30, 10)
+    yield "planted_wide", (np.concatenate([u, u2]), np.concatenate([v, v2]))
+    u, v = engine.gen_planted(600, 8, 50, 70, 11)
+    u2, v2 = engine.gen_gnp(600, 20, 12)
+    yield "planted_mid", (np.concatenate([u, u2]), np.concatenate([v, v2]))
+
+
+CASE_NAMES = ["chung_lu_1e4", "rmat12", "rmat13_ef8", "gnp400_0", "gnp400_1", "gnp400_2", "planted_wide",
+              "planted_mid"]
+
+
+@pytest.mark.parametrize("name", CASE_NAMES)
+def test_against_oracle(gpu, oracle_mod, name):
+    u, v = dict(_cases(gpu))[name]
+    og, o = oracle_result(oracle_mod, u, v)
+    with gpu.Graph.from_coo(u, v, opts(gpu)) as g:
+        r = g.solve(opts(gpu))
+        assert (r.num_vertices, r.num_edges, r.degeneracy, r.max_degree) == (og.n, og.m, og.degeneracy,
+                                                                             og.max_degree)
+    assert_same(r, o, name)
+
+
+def test_rmat14_all_modes(gpu, oracle_mod):
+    u, v = gpu.gen_rmat(14, 16, 1)
+    _, o = oracle_result(oracle_mod, u, v)
+    assert o.count == 107790386
+    with gpu.Graph.from_coo(u, v, opts(gpu)) as g:
+        assert_same(g.solve(opts(gpu)), o, "sharing")
+        assert_same(g.solve(opts(gpu)), o, "repeat")
+        assert_same(g.solve(opts(gpu, flags=gpu.FLAG_NO_SHARING)), o, "no sharing")
+        assert_same(g.solve(opts(gpu, expand_r=0)), o, "no EXPAND_R")
+        assert_same(g.solve(opts(gpu, share_bound=4)), o, "share bound 4")
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+def test_vertex_orders(gpu, oracle_mod, order):
+    u, v = gpu.gen_rmat(12, 16, 3)
+    _, o = oracle_result(oracle_mod, u, v)
+    with gpu.Graph.from_coo(u, v, opts(gpu, order=order)) as g:
+        assert_same(g.solve(opts(gpu)), o, f"order {order}")
+
+
+def test_degeneracy_order_is_valid(gpu, oracle_mod):
+    u, v = gpu.gen_rmat(13, 16, 7)
+    og = oracle_mod.Graph.from_pairs(u, v)
+    core = og.core_numbers()
+    og.sort_degeneracy()
+    with gpu.Graph.from_coo(u, v, opts(gpu)) as g:
+        ro, ci, lab = g.export_csr()
+        k = g.info()["degeneracy"]
+    assert k == int(core.max()) == og.degeneracy
+    n = len(ro) - 1
+    ro = ro.astype(np.int64)
+    later = np.zeros(n, np.int64)
+    for x in range(n):
+        row = ci[ro[x]:ro[x + 1]]
+        assert np.all(np.diff(row.astype(np.int64)) > 0)
+        later[x] = int((row > x).sum())
+    assert later.max() <= k
+    _, _, olab = og.export()
+    assert np.array_equal(np.sort(lab), np.sort(olab))
+
+
+def test_sampled_roots_rmat16(gpu, oracle_mod):
+    u, v = gpu.gen_rmat(16, 16, 1)
+    og = oracle_mod.Graph.from_pairs(u, v).sort_degeneracy()
+    rng = np.random.default_rng(7)
+    roots = np.sort(rng.choice(og.m, 400, replace=False)).astype(np.uint64)
+    ocnt, ochk = og.mce_roots(roots, threads=THREADS)
+    with gpu.Graph.from_coo(u, v, opts(gpu)) as g:
+        light = roots[ocnt < 2_000_000]
+        cnt, chk = g.solve_roots(light, opts(gpu))
+        keep = ocnt < 2_000_000
+        assert np.array_equal(cnt, ocnt[keep]) and np.array_equal(chk, ochk[keep])
+        r = g.solve_root_list(roots, opts(gpu))
+    assert r.count == int(ocnt.sum())
+    assert r.checksum == int(ochk.sum(dtype=np.uint64))
+    assert r.roots == len(roots)
+
+
+def test_root_ranges_partition(gpu, oracle_mod):
+    u, v = gpu.gen_rmat(13, 16, 2)
+    _, o = oracle_result(oracle_mod, u, v)
+    with gpu.Graph.from_coo(u, v, opts(gpu)) as g:
+        m = g.info()["num_edges"]
+        cuts = [0, m // 7, m // 2, m - 3, m]
+        tot, chk = 0, 0
+        hist = {}
+        for a, b in zip(cuts[:-1], cuts[1:]):
+            r = g.solve(opts(gpu, root_begin=a, root_end=b))
+            tot += r.count
+            chk = (chk + r.checksum) % (1 << 64)
+            for s, c in r.hist.items():
+                hist[s] = hist.get(s, 0) + c
+    assert (tot, chk, hist) == (o.count, o.checksum, o.hist)
+
+
+def tier_graph(p_cols, x_rows, seed=5):
+    """Under the unchanged order, the root edge (x_rows, x_rows + 1) has exactly
+    p_cols candidate columns and up to x_rows X rows."""
+    rng = np.random.default_rng(seed)
+    X = np.arange(x_rows)
+    v0, v1 = x_rows, x_rows + 1
+    P = np.arange(x_rows + 2, x_rows + 2 + p_cols)
+    e = [(v0, v1)]
+    e += [(v0, int(x)) for x in X] + [(v1, int(x)) for x in X]
+    e += [(v0, int(p)) for p in P] + [(v1, int(p)) for p in P]
+    for i in range(p_cols):
+        for j in range(i + 1, p_cols):
+            if rng.random() < 0.5:
+                e.append((int(P[i]), int(P[j])))
+    for x in X:
+        for p in P:
+            if rng.random() < 0.5:
+                e.append((int(x), int(p)))
+    a = np.array(e, np.uint32)
+    return a[:, 0].copy(), a[:, 1].copy()
+
+
+@pytest.mark.parametrize("p_cols,x_rows", [(63, 0), (64, 0), (65, 0), (64, 64), (60, 68), (60, 69), (127, 3),
+                                           (128, 10), (129, 40)])
+@pytest.mark.parametrize("sharing", [True, False])
+def test_tier_boundaries(gpu, oracle_mod, p_cols, x_rows, sharing):
+    u, v = tier_graph(p_cols, x_rows)
+    _, o = oracle_result(oracle_mod, u, v)
+    flags = 0 if sharing else gpu.FLAG_NO_SHARING
+    with gpu.Graph.from_coo(u, v, opts(gpu, order=gpu.ORDER_UNCHANGED)) as g:
+        r = g.solve(opts(gpu, flags=flags, share_bound=4))
+    assert_same(r, o, f"{p_cols}x{x_rows}")
+
+
+def test_edge_cases(gpu):
+    o = opts(gpu)
+    r = gpu.solve_coo(np.array([7], np.uint32), np.array([9], np.uint32), o)
+    assert (r.count, r.hist) == (1, {2: 1})
+    r = gpu.solve_coo(np.array([3, 4], np.uint32), np.array([3, 4], np.uint32), o)
+    assert (r.count, r.num_vertices) == (0, 0)
+    r = gpu.solve_coo(np.zeros(0, np.uint32), np.zeros(0, np.uint32), o)
+    assert r.count == 0
+    u = np.array([1, 2, 2, 1, 3, 3, 1], np.uint32)
+    v = np.array([2, 1, 3, 3, 1, 2, 2], np.uint32)
+    r = gpu.solve_coo(u, v, o)
+    assert (r.count, r.hist, r.num_edges) == (1, {3: 1}, 3)
+
+
+def test_bin_roundtrip(gpu, oracle_mod, tmp_path):
+    u, v = gpu.gen_rmat(11, 16, 3)
+    path = str(tmp_path / "g.bin")
+    with gpu.Graph.from_coo(u, v, opts(gpu)) as g:
+        r1 = g.solve(opts(gpu))
+        g.store_bin(path)
+    with gpu.Graph.load_file(path, opts(gpu)) as h:
+        r2 = h.solve(opts(gpu))
+    assert_same(r2, r1)
+    oh = oracle_mod.Graph.load_bin(path)
+    assert oh.mce(threads=THREADS).count == r1.count
