@@ -6,18 +6,20 @@
 //   Graph::SortByDegeneracy/ApplyOrder  src/graph.cc:333-358, 54-77
 //   Graph::ConvertToCsr + LoadFromCpu   src/graph.cc:268-288, src/graph_gpu.cu:3-58
 // Steps: pack (min,max) keys -> radix sort -> unique -> mark/scan dense ids ->
-// degrees -> level-synchronous k-core peeling (one persistent launch per level,
-// cascade through a device queue) -> relabel both edge directions -> radix sort
-// -> CSR offsets by scan -> root list (v0 < v1) by flag+scan.
-// The peel order inside a level differs from the reference's scan+BFS order;
-// any peeling order gives the same degeneracy value and the same clique set.
+// degrees -> k-core peeling in synchronous rounds (one cooperative launch) ->
+// relabel both edge directions -> radix sort -> CSR offsets by scan -> root
+// list (v0 < v1) by flag+scan.
 #include <algorithm>
 #include <vector>
+
+#include <cooperative_groups.h>
 
 #include "common.cuh"
 #include "engine.h"
 
 namespace mce {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -92,126 +94,125 @@ __global__ void k_iota(uint32_t *a, uint64_t n) {
     a[i] = (uint32_t)i;
 }
 
-// ---- k-core peeling: one persistent launch per level k ----
+// ---- k-core peeling in synchronous rounds (one cooperative launch) ----
+//
+// Level k: the frontier F_0 = unremoved vertices of residual degree <= k; each
+// round removes its whole frontier at once and decrements the neighbours, and
+// every neighbour that drops to k joins the next round's frontier.  A vertex's
+// position is (global round, vertex id): every later neighbour of x is either
+// in x's round or in a later one, all of which were unremoved when x's
+// residual degree fell to <= k, so x has at most k later neighbours -- a
+// degeneracy order.  The rounds make the order deterministic, so root ids
+// (edges of the ordered CSR) are stable from run to run; the reference's
+// sequential queue (graph.cc:341-356) orders vertices inside a round
+// differently, which changes neither the degeneracy nor the clique set.
 struct PeelCtl {
-  uint32_t tail;       // entries appended to order[]
-  uint32_t head;       // next order[] entry to take
-  uint32_t processed;  // entries whose neighbours were decremented
-  uint32_t scan_done;  // scan chunks finished
-  uint32_t scan_next;  // next scan chunk to claim
-  uint32_t next_n;     // survivors appended to the next remaining list
-  uint32_t min_rest;   // smallest degree > k seen among unclaimed vertices
-  uint32_t claimed;    // claims at this level
-  uint32_t error;      // nonzero: a bounded wait expired
+  uint32_t fcnt[3];     // frontier sizes, by round mod 3
+  uint32_t rcnt[3];     // survivors of each level's scan, by level mod 3
+  uint32_t rmin[3];     // smallest surviving residual degree, by level mod 3
+  uint32_t degeneracy;
+  uint32_t rounds;
+  uint32_t levels;
+  uint32_t error;       // 1: level bound exceeded (cannot happen on a consistent CSR)
 };
 
-__device__ __forceinline__ void peel_claim(uint32_t v, uint32_t *state, uint32_t *order, PeelCtl *ctl) {
-  if (atomicCAS(&state[v], 0u, 1u) == 0u) {
-    uint32_t p = atomicAdd(&ctl->tail, 1u);
-    atomicAdd(&ctl->claimed, 1u);
-    volatile uint32_t *o = order;
-    o[p] = v;
-  }
-}
-
-constexpr uint32_t kPeelChunk = 1024;
-
-// Termination never assumes all warps run at once: the scan is handed out in
-// chunks, and a level is finished when every chunk is scanned and every
-// claimed vertex is processed.
-__global__ void __launch_bounds__(256) k_peel_level(uint32_t k, const uint32_t *rem, uint32_t nrem,
-                                                    uint32_t *rem_next, const uint32_t *off,
-                                                    const uint32_t *adj, int *deg, uint32_t *state,
-                                                    uint32_t *order, PeelCtl *ctl, uint32_t nchunks,
-                                                    uint64_t spin_limit) {
-  const uint32_t lane = lane_id();
-  // 1) scan the remaining vertices: claim degree <= k, keep the rest
-  uint32_t local_min = 0xffffffffu;
-  for (;;) {
-    uint32_t ch = 0;
-    if (lane == 0) ch = atomicAdd(&ctl->scan_next, 1u);
-    ch = __shfl_sync(kFull, ch, 0);
-    if (ch >= nchunks) break;
-    const uint32_t end = min(nrem, (ch + 1) * kPeelChunk);
-    for (uint32_t i = ch * kPeelChunk + lane; i < end; i += 32) {
-      const uint32_t v = rem[i];
-      if (state[v] != 0) continue;
-      const int d = deg[v];
+__global__ void __launch_bounds__(256) k_peel_rounds(uint32_t n, const uint32_t *off, const uint32_t *adj,
+                                                     int *deg, uint32_t *state, uint32_t *remA, uint32_t *remB,
+                                                     uint32_t *frA, uint32_t *frB, PeelCtl *ctl, uint32_t max_levels) {
+  cg::grid_group grid = cg::this_grid();
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t gwarp = tid >> 5, nwarps = nthreads >> 5;
+  const bool leader = tid == 0;
+  uint32_t k = 0, degen = 0, lev = 0, r = 0, removed = 0, nrem = n;
+  uint32_t *rem_cur = remA, *rem_nxt = remB;
+  while (removed < n) {
+    if (lev > max_levels) {
+      if (leader) atomicExch(&ctl->error, 1u);
+      break;  // uniform: every thread sees the same lev
+    }
+    uint32_t *fr = (r & 1) ? frB : frA;
+    // scan: claim residual degree <= k into F_r, keep the rest
+    if (leader) {
+      ctl->rcnt[(lev + 1) % 3] = 0;
+      ctl->rmin[(lev + 1) % 3] = 0xffffffffu;
+    }
+    uint32_t local_min = 0xffffffffu;
+    for (uint64_t i = tid; i < nrem; i += nthreads) {
+      const uint32_t v = __ldcg(rem_cur + i);
+      if (__ldcg(state + v)) continue;
+      const int d = __ldcg(deg + v);
       if (d <= (int)k) {
-        peel_claim(v, state, order, ctl);
+        state[v] = r + 1;
+        fr[atomicAdd(&ctl->fcnt[r % 3], 1u)] = v;
       } else {
-        rem_next[atomicAdd(&ctl->next_n, 1u)] = v;
+        rem_nxt[atomicAdd(&ctl->rcnt[lev % 3], 1u)] = v;
         local_min = min(local_min, (uint32_t)d);
       }
     }
-    __syncwarp();
-    if (lane == 0) {
-      __threadfence();
-      atomicAdd(&ctl->scan_done, 1u);
-    }
-  }
-  local_min = __reduce_min_sync(kFull, local_min);
-  if (lane == 0 && local_min != 0xffffffffu) atomicMin(&ctl->min_rest, local_min);
-  // 2) cascade: process claimed vertices through the order[] queue
-  volatile PeelCtl *vc = ctl;
-  volatile uint32_t *vorder = order;
-  uint64_t spins = 0;
-  for (;;) {
-    uint32_t idx = 0;
-    if (lane == 0) idx = atomicAdd(&ctl->head, 1u);
-    idx = __shfl_sync(kFull, idx, 0);
-    // wait until idx is claimed, or the level is finished
-    bool have = false;
+    local_min = __reduce_min_sync(kFull, local_min);
+    if (lane == 0 && local_min != 0xffffffffu) atomicMin(&ctl->rmin[lev % 3], local_min);
+    grid.sync();
+    uint32_t level_claims = 0;
     for (;;) {
-      uint32_t t = 0, done = 0, sd = 0;
-      if (lane == 0) {
-        // order matters: scans finished, then processed, then tail.  processed
-        // never exceeds tail, so processed == tail read in this order means no
-        // entry was in flight and no claim can follow.
-        sd = vc->scan_done;
-        __threadfence();
-        done = vc->processed;
-        __threadfence();
-        t = vc->tail;
-      }
-      t = __shfl_sync(kFull, t, 0);
-      sd = __shfl_sync(kFull, sd, 0);
-      done = __shfl_sync(kFull, done, 0);
-      if (idx < t) {
-        have = true;
-        break;
-      }
-      if (sd == nchunks && done == t) break;  // no claim can arrive any more
-      if (++spins > spin_limit) {
-        if (lane == 0) atomicExch(&ctl->error, 1u);
-        return;
-      }
-      __nanosleep(200);
-    }
-    if (!have) return;
-    uint32_t v = 0xffffffffu;
-    if (lane == 0) {
-      while ((v = vorder[idx]) == 0xffffffffu) {
-        if (++spins > spin_limit) {
-          atomicExch(&ctl->error, 1u);
-          break;
+      const uint32_t nf = __ldcg(&ctl->fcnt[r % 3]);
+      if (nf == 0) break;
+      level_claims += nf;
+      removed += nf;
+      const uint32_t *cur = (r & 1) ? frB : frA;
+      uint32_t *nxt = (r & 1) ? frA : frB;
+      if (leader) ctl->fcnt[(r + 2) % 3] = 0;  // last read in round r - 1
+      for (uint64_t i = gwarp; i < nf; i += nwarps) {
+        const uint32_t v = __ldcg(cur + i);
+        const uint32_t e1 = off[v + 1];
+        for (uint32_t e = off[v] + lane; e < e1; e += 32) {
+          const uint32_t u = adj[e];
+          if (__ldcg(state + u)) continue;
+          if (atomicSub(&deg[u], 1) == (int)k + 1 && atomicCAS(&state[u], 0u, r + 2) == 0u)
+            nxt[atomicAdd(&ctl->fcnt[(r + 1) % 3], 1u)] = u;
         }
       }
+      grid.sync();
+      r++;
     }
-    v = __shfl_sync(kFull, v, 0);
-    if (v == 0xffffffffu) return;
-    for (uint32_t e = off[v] + lane; e < off[v + 1]; e += 32) {
-      uint32_t u = adj[e];
-      if (state[u] != 0) continue;
-      int old = atomicSub(&deg[u], 1);
-      if (old == (int)k + 1) peel_claim(u, state, order, ctl);
+    // F_r is empty: round index r is skipped, so no vertex of the next level
+    // shares a round number with this level's
+    r++;
+    nrem = __ldcg(&ctl->rcnt[lev % 3]);
+    const uint32_t rmin = __ldcg(&ctl->rmin[lev % 3]);
+    uint32_t *t = rem_cur;
+    rem_cur = rem_nxt;
+    rem_nxt = t;
+    if (level_claims) {
+      degen = k;
+      k = k + 1;
+    } else {
+      if (rmin == 0xffffffffu) break;
+      k = max(k + 1, rmin);
     }
-    __syncwarp();
-    if (lane == 0) {
-      __threadfence();
-      atomicAdd(&ctl->processed, 1u);
-    }
+    lev++;
+    // The next scan fills fcnt[r % 3] and the round after it fcnt[(r + 1) % 3],
+    // which still holds the size of this level's last processed round; the
+    // only counter still being read (fcnt of the empty round) is already zero.
+    if (leader) ctl->fcnt[0] = ctl->fcnt[1] = ctl->fcnt[2] = 0;
+    grid.sync();
   }
+  if (leader) {
+    ctl->degeneracy = degen;
+    ctl->rounds = r;
+    ctl->levels = lev;
+  }
+}
+
+__global__ void k_round_keys(const uint32_t *state, uint32_t n, int nb, uint64_t *keys) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    keys[i] = ((uint64_t)(state[i] - 1) << nb) | i;
+}
+
+__global__ void k_order_from_round_keys(const uint64_t *keys, uint32_t n, uint64_t mask, uint32_t *order) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    order[i] = (uint32_t)(keys[i] & mask);
 }
 
 __global__ void k_rank_from_order(const uint32_t *order, uint32_t n, uint32_t *rank) {
@@ -306,75 +307,61 @@ mce_status read_scalar(const T *d, T *h, cudaStream_t st) {
 }
 
 // k-core peeling over an unsorted symmetric CSR; fills order[] (position -> vertex)
-mce_status peel(uint32_t n, const uint32_t *off, const uint32_t *adj, const uint32_t *deg0, uint32_t *order,
-                uint32_t *degeneracy, uint64_t spin_limit, cudaStream_t st) {
+mce_status peel(uint32_t n, const uint32_t *off, const uint32_t *adj, const uint32_t *deg0, uint32_t max_degree,
+                uint32_t *order, uint32_t *degeneracy, cudaStream_t st) {
   DevBuf<int> deg;
-  DevBuf<uint32_t> state, remA, remB;
+  DevBuf<uint32_t> state, remA, remB, frA, frB;
   DevBuf<PeelCtl> ctl;
   MCE_TRY(deg.alloc(n, st));
   MCE_TRY(state.alloc(n, st));
   MCE_TRY(remA.alloc(n, st));
   MCE_TRY(remB.alloc(n, st));
+  MCE_TRY(frA.alloc(n, st));
+  MCE_TRY(frB.alloc(n, st));
   MCE_TRY(ctl.alloc(1, st));
   MCE_CUDA_TRY(cudaMemcpyAsync(deg.p, deg0, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
   MCE_CUDA_TRY(cudaMemsetAsync(state.p, 0, n * sizeof(uint32_t), st));
-  MCE_CUDA_TRY(cudaMemsetAsync(order, 0xff, n * sizeof(uint32_t), st));
   k_iota<<<grid_for(n, 256), 256, 0, st>>>(remA.p, n); note_launch();
-  int dev = 0;
-  MCE_CUDA_TRY(cudaGetDevice(&dev));
-  int sms = 0, per_sm = 0;
-  MCE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  MCE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel_level, 256, 0));
-  // every block must be resident: waiting warps spin on work other warps produce
-  uint32_t blocks = (uint32_t)std::max(1, std::min(per_sm, 4)) * (uint32_t)sms;
   PeelCtl h{};
-  uint32_t nrem = n, tail = 0, k = 0, degen = 0;
+  for (int i = 0; i < 3; i++) h.rmin[i] = 0xffffffffu;
   PeelCtl *hc = nullptr;
   MCE_CUDA_TRY(cudaMallocHost(&hc, sizeof(PeelCtl)));
-  mce_status s = MCE_OK;
-  while (tail < n) {
-    h = PeelCtl{};
-    h.tail = tail;
-    h.head = tail;
-    h.processed = tail;
-    h.min_rest = 0xffffffffu;
-    *hc = h;
-    if (cudaMemcpyAsync(ctl.p, hc, sizeof(PeelCtl), cudaMemcpyHostToDevice, st) != cudaSuccess) {
-      s = MCE_ERR_CUDA;
-      break;
-    }
-    const uint32_t nchunks = (nrem + kPeelChunk - 1) / kPeelChunk;
-    k_peel_level<<<blocks, 256, 0, st>>>(k, remA.p, nrem, remB.p, off, adj, deg.p, state.p, order, ctl.p,
-                                          nchunks, spin_limit); note_launch();
-    if (cudaGetLastError() != cudaSuccess) {
-      s = MCE_ERR_CUDA;
-      break;
-    }
-    if (cudaMemcpyAsync(hc, ctl.p, sizeof(PeelCtl), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess) {
-      s = MCE_ERR_CUDA;
-      break;
-    }
-    h = *hc;
-    if (h.error) {
-      s = MCE_ERR_TIMEOUT;
-      break;
-    }
-    tail = h.tail;
-    nrem = h.next_n;
-    std::swap(remA.p, remB.p);
-    if (h.claimed) {
-      degen = k;
-      k = k + 1;
-    } else {
-      if (h.min_rest == 0xffffffffu) break;
-      k = std::max(k + 1, h.min_rest);
-    }
-  }
-  cudaFreeHost(hc);
-  if (s == MCE_OK && tail != n) s = MCE_ERR_INTERNAL;
-  *degeneracy = degen;
-  return s;
+  struct FreeHost {
+    void *p;
+    ~FreeHost() { cudaFreeHost(p); }
+  } free_hc{hc};
+  *hc = h;
+  MCE_CUDA_TRY(cudaMemcpyAsync(ctl.p, hc, sizeof(PeelCtl), cudaMemcpyHostToDevice, st));
+  int dev = 0, sms = 0, per_sm = 0;
+  MCE_CUDA_TRY(cudaGetDevice(&dev));
+  MCE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  MCE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel_rounds, 256, 0));
+  if (per_sm < 1) return MCE_ERR_INTERNAL;
+  // a cooperative launch: every block is resident, so grid.sync() is sound
+  const uint32_t blocks = (uint32_t)std::min(per_sm, 2) * (uint32_t)sms;
+  uint32_t nn = n, maxl = max_degree + 2;
+  int *degp = deg.p;
+  uint32_t *statep = state.p, *ra = remA.p, *rb = remB.p, *fa = frA.p, *fb = frB.p;
+  PeelCtl *cp = ctl.p;
+  void *args[] = {&nn, (void *)&off, (void *)&adj, &degp, &statep, &ra, &rb, &fa, &fb, &cp, &maxl};
+  MCE_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)k_peel_rounds, dim3(blocks), dim3(256), args, 0, st));
+  note_launch();
+  MCE_CUDA_TRY(cudaMemcpyAsync(hc, ctl.p, sizeof(PeelCtl), cudaMemcpyDeviceToHost, st));
+  MCE_CUDA_TRY(cudaStreamSynchronize(st));
+  h = *hc;
+  if (h.error) return MCE_ERR_INTERNAL;
+  *degeneracy = h.degeneracy;
+  // order = vertices sorted by (round, id)
+  const int nb = bits_for(n ? n - 1 : 0), rb_bits = bits_for(h.rounds);
+  if (nb + rb_bits > 64) return MCE_ERR_TOO_LARGE;
+  DevBuf<uint64_t> keys, tmp;
+  MCE_TRY(keys.alloc(n, st));
+  MCE_TRY(tmp.alloc(n, st));
+  k_round_keys<<<grid_for(n, 256), 256, 0, st>>>(state.p, n, nb, keys.p); note_launch();
+  MCE_TRY(radix_sort_u64(keys.p, tmp.p, n, nb + rb_bits, st));
+  k_order_from_round_keys<<<grid_for(n, 256), 256, 0, st>>>(keys.p, n, (1ULL << nb) - 1, order); note_launch();
+  MCE_CUDA_TRY(cudaGetLastError());
+  return MCE_OK;
 }
 
 }  // namespace
@@ -582,7 +569,7 @@ mce_status finish_graph(uint32_t n, uint64_t m, const uint32_t *eu, const uint32
     MCE_TRY(scan_exclusive_u32(deg, off0.p, n, off0.p + n, st));
     MCE_CUDA_TRY(cudaMemcpyAsync(cursor.p, off0.p, (n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     k_fill_adj<<<grid_for(m, 256), 256, 0, st>>>(eu, ev, m, cursor.p, adj0.p); note_launch();
-    MCE_TRY(peel(n, off0.p, adj0.p, deg, order.p, &g->degeneracy, spin_limit, st));
+    MCE_TRY(peel(n, off0.p, adj0.p, deg, g->max_degree, order.p, &g->degeneracy, st));
   } else if ((order_kind == MCE_ORDER_DEGREE_ASC || order_kind == MCE_ORDER_DEGREE_DESC) && n > 0) {
     DevBuf<uint64_t> dk, dt;
     MCE_TRY(dk.alloc(n, st));

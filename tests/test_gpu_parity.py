@@ -116,13 +116,31 @@ def test_degeneracy_order_is_valid(gpu, oracle_mod):
     assert np.array_equal(np.sort(lab), np.sort(olab))
 
 
+def test_order_is_deterministic(gpu):
+    """Root ids are edges of the ordered CSR: the same input must give the same
+    CSR every time, on the dense- and the sparse-label relabel paths."""
+    u, v = gpu.gen_rmat(15, 16, 4)
+    for uu, vv in [(u, v), (u * np.uint32(4001) + np.uint32(7), v * np.uint32(4001) + np.uint32(7))]:
+        outs = []
+        for _ in range(3):
+            with gpu.Graph.from_coo(uu, vv, opts(gpu)) as g:
+                outs.append(g.export_csr())
+        for o in outs[1:]:
+            assert all(np.array_equal(a, b) for a, b in zip(outs[0], o))
+
+
 def test_sampled_roots_rmat16(gpu, oracle_mod):
+    """Per-root counts and checksums.  Root r is the r-th edge (v0 < v1) of the
+    ordered CSR; the GPU peel orders vertices within a k-core level differently
+    from the reference's sequential queue, so the oracle is handed the GPU's
+    ordered CSR (whose validity test_degeneracy_order_is_valid checks)."""
     u, v = gpu.gen_rmat(16, 16, 1)
-    og = oracle_mod.Graph.from_pairs(u, v).sort_degeneracy()
-    rng = np.random.default_rng(7)
-    roots = np.sort(rng.choice(og.m, 400, replace=False)).astype(np.uint64)
-    ocnt, ochk = og.mce_roots(roots, threads=THREADS)
     with gpu.Graph.from_coo(u, v, opts(gpu)) as g:
+        ro, ci, lab = g.export_csr()
+        og = oracle_mod.Graph.from_csr(ro.astype(np.uint64), ci, lab)
+        rng = np.random.default_rng(7)
+        roots = np.sort(rng.choice(og.m, 400, replace=False)).astype(np.uint64)
+        ocnt, ochk = og.mce_roots(roots, threads=THREADS)
         light = roots[ocnt < 2_000_000]
         cnt, chk = g.solve_roots(light, opts(gpu))
         keep = ocnt < 2_000_000
