@@ -38,13 +38,18 @@ sys.path.insert(0, ROOT)
 
 SCALE, EDGE_FACTOR, GRAPH_SEED = 20, 16, 2
 SAMPLE_SEED = 12345
+# smaller graphs enumerated in full (profiling and context lines): name -> (scale, edge factor, seed)
+FULL_WORKLOADS = {"rmat14": (14, 16, 1), "rmat16": (16, 16, 1)}
 DEFAULT_SAMPLE = int(os.environ.get("RDMCE_BENCH_SAMPLE", "256"))
 METRIC = "maximal cliques/s"
 UNIT = "cliques/s"
 REF_CPU = os.path.join(ROOT, "oracle", "_ref", "ref_cpu")
 
 
-def workload_name(sample):
+def workload_name(sample, workload="rmat20-sample"):
+    if workload in FULL_WORKLOADS:
+        sc, ef, sd = FULL_WORKLOADS[workload]
+        return f"R-MAT scale {sc}, edge factor {ef}, a/b/c/d=0.57/0.19/0.19/0.05, seed {sd}; full enumeration"
     return (f"R-MAT scale {SCALE}, edge factor {EDGE_FACTOR}, a/b/c/d=0.57/0.19/0.19/0.05, seed {GRAPH_SEED}; "
             f"all maximal cliques under {sample} seeded random edge roots per rank per step")
 
@@ -106,9 +111,12 @@ def dist_env():
     return rank, world, local
 
 
-def make_graph_pairs():
+def make_graph_pairs(workload="rmat20-sample"):
     import rdmce_b200 as mce
 
+    if workload in FULL_WORKLOADS:
+        sc, ef, sd = FULL_WORKLOADS[workload]
+        return mce.gen_rmat(sc, ef, sd)
     return mce.gen_rmat(SCALE, EDGE_FACTOR, GRAPH_SEED)
 
 
@@ -231,10 +239,16 @@ def run_ours(args):
 
     stream = torch.cuda.current_stream(dev)
     o = mce.options(device=local, stream=C.c_void_p(stream.cuda_stream))
-    u, v = make_graph_pairs()
+    full = args.workload in FULL_WORKLOADS
+    u, v = make_graph_pairs(args.workload)
     g = mce.Graph.from_coo(u, v, o)
     info = g.info()
-    roots = root_sample(info["num_edges"], args.sample, rank)
+    if full:
+        # every root; ranks split the edge list into contiguous ranges
+        roots = np.arange(info["num_edges"] * rank // world, info["num_edges"] * (rank + 1) // world,
+                          dtype=np.uint64)
+    else:
+        roots = root_sample(info["num_edges"], args.sample, rank)
 
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)  # 4x L2
 
@@ -243,7 +257,7 @@ def run_ours(args):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        r = g.solve_root_list(roots, o)
+        r = g.solve(o) if full and world == 1 else g.solve_root_list(roots, o)
         e1.record(stream)
         e1.synchronize()
         return r, e0.elapsed_time(e1)
@@ -298,7 +312,10 @@ def run_ours(args):
                                  C.byref(h))
         if s != mce.OK:
             raise mce.MceError(s, "mce_graph_from_coo")
-        s = L.mce_solve_root_list(h, C.c_void_p(roots_pin.data_ptr()), len(roots), C.byref(o), C.byref(res))
+        if full and world == 1:
+            s = L.mce_solve(h, C.byref(o), C.byref(res))
+        else:
+            s = L.mce_solve_root_list(h, C.c_void_p(roots_pin.data_ptr()), len(roots), C.byref(o), C.byref(res))
         e1.record(stream)
         e1.synchronize()
         L.mce_graph_free(h)
@@ -325,7 +342,7 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": workload_name(args.sample), "roots_per_step": int(len(roots)),
+            "config": {"workload": workload_name(args.sample, args.workload), "roots_per_step": int(len(roots)),
                        "sample_seed": SAMPLE_SEED, "vertices": info["num_vertices"], "edges": info["num_edges"],
                        "degeneracy": info["degeneracy"], "max_degree": info["max_degree"],
                        "cliques_per_step": int(ref[0]), "checksum": f"{ref[1]:016x}",
@@ -336,7 +353,8 @@ def run_ours(args):
                          "note": "64-bit bitmap row word-ops (ANDN+POPC per active row per node, row filters) of "
                                  "k_enumerate / its event-timed duration; peak = live INT-pipe probe of the same "
                                  "op mix on this GPU"},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(u.nbytes + v.nbytes + roots.nbytes),
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": int(u.nbytes + v.nbytes + (0 if full and world == 1 else roots.nbytes)),
                     "d2h_bytes_per_step": int(C.sizeof(mce._Result))},
             "gpu_launches": int(launches),
             "clocks": clk,
@@ -377,6 +395,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--sample", type=int, default=DEFAULT_SAMPLE, help="edge roots per rank per step")
+    ap.add_argument("--workload", choices=["rmat20-sample"] + sorted(FULL_WORKLOADS), default="rmat20-sample",
+                    help="the headline root sample of R-MAT scale 20, or a smaller graph enumerated in full")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU oracle time bound (0 = skip)")
     args = ap.parse_args()
     if args.warmup < 3:
