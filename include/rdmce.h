@@ -18,7 +18,7 @@
  *     MCE_ERR_TIMEOUT and leaves the CUDA context usable.
  *   - Vertex labels are the caller's uint32 ids.  Isolated vertices and
  *     vertices with only self-loops are dropped, as the reference loader does
- *     (src/graph.cc:140-181); every reported clique therefore has size >= 2.
+ *     (src/graph.cc:64-152); every reported clique therefore has size >= 2.
  *   - Results are exact: count, clique-size histogram and a 64-bit checksum
  *     = sum over cliques C (mod 2^64) of mix64(s1 ^ rotl(s2,31) ^ (|C| << 56)),
  *     s1 = sum mix64(l), s2 = sum mix64(l ^ 0x9E3779B97F4A7C15) over the
@@ -123,7 +123,7 @@ mce_status mce_probe_int_peak(int device, double *word_ops_per_s);
 
 /* COO pairs in host memory -> device-resident, degeneracy-ordered CSR.
  * Replaces Graph::LoadFromFile's edge handling + SortByOrder + ConvertToCsr +
- * GraphGpu::LoadFromCpu (src/graph.cc:116-204, 333-358, 268-288;
+ * GraphGpu::LoadFromCpu (src/graph.cc:64-152, 281-306, 216-236;
  * src/graph_gpu.cu:3-58); here sort, dedup, relabel and k-core peeling run on
  * the GPU. */
 mce_status mce_graph_from_coo(const uint32_t *u, const uint32_t *v, uint64_t n_pairs,
@@ -134,19 +134,19 @@ mce_status mce_graph_from_coo_device(const uint32_t *u_device, const uint32_t *v
                                      const mce_options *opt, mce_graph **out);
 
 /* A symmetric CSR with sorted rows (uint32 offsets, as Graph::ConvertToCsr
- * builds, src/graph.cc:268-288).  labels may be NULL (label = id).  If
+ * builds, src/graph.cc:216-236).  labels may be NULL (label = id).  If
  * already_ordered is nonzero the rows are used as given (as main.cc:26 does for
  * .bin input); otherwise the graph is reordered by `opt->order`. */
 mce_status mce_graph_from_csr(uint64_t n, const uint32_t *rowoffset, const uint32_t *colidx,
                               const uint32_t *labels, int already_ordered, const mce_options *opt,
                               mce_graph **out);
 
-/* COO text (Graph::LoadFromFile, src/graph.cc:116-204) or the reference .bin
- * container (Graph::LoadFromBin, src/graph.cc:230-265), chosen by the .bin
+/* COO text (Graph::LoadFromFile, src/graph.cc:64-152) or the reference .bin
+ * container (Graph::LoadFromBin, src/graph.cc:178-213), chosen by the .bin
  * suffix exactly as main.cc:181-191 does. */
 mce_status mce_graph_load_file(const char *path, const mce_options *opt, mce_graph **out);
 
-/* Write the reference .bin container (Graph::StoreIntoBin, src/graph.cc:206-228). */
+/* Write the reference .bin container (Graph::StoreIntoBin, src/graph.cc:154-176). */
 mce_status mce_graph_store_bin(const mce_graph *g, const char *path);
 
 mce_status mce_graph_info_get(const mce_graph *g, mce_graph_info *info);
@@ -229,7 +229,7 @@ mce_status mce_gen_planted(uint32_t n, uint32_t num_cliques, uint32_t size_lo, u
 mce_status mce_gen_batch_member(uint32_t index, uint64_t base_seed, uint32_t *u, uint32_t *v,
                                 uint64_t capacity, uint64_t *out_count, uint32_t *out_n);
 
-/* COO text parse with the reference's istream semantics (src/graph.cc:134-156).
+/* COO text parse with the reference's istream semantics (src/graph.cc:82-104).
  * Buffers are malloc'ed; release them with mce_free_host. */
 mce_status mce_parse_text(const char *path, uint32_t **u, uint32_t **v, uint64_t *n_pairs);
 void mce_free_host(void *p);

@@ -5,10 +5,10 @@
  * this code, as the checker.  The product (rdmce_b200/) never links it.
  *
  * What it restates (reference paths relative to the RDMCE project root):
- *   - text parse:        src/graph.cc:134-156  (istream >> u >> v, bad lines skipped)
- *   - loader rules:      src/graph.cc:140-204  (self-loops dropped, u<v, sort+unique,
+ *   - text parse:        src/graph.cc:82-104  (istream >> u >> v, bad lines skipped)
+ *   - loader rules:      src/graph.cc:64-152  (self-loops dropped, u<v, sort+unique,
  *                                               dense relabel of present labels)
- *   - degeneracy order:  src/graph.cc:333-358 + ApplyOrder src/graph.cc:54-77
+ *   - degeneracy order:  src/graph.cc:281-306 + ApplyOrder src/graph.cc:2-25
  *   - edge roots:        src/kernels/BkPivotBitBalance.cuh:428-469 (v0<v1, P = common
  *                        neighbours > v1, X = common neighbours < v1; an edge in no
  *                        triangle is a clique of size 2, :535-539)
@@ -18,7 +18,7 @@
  *                        rows containing R of |P \ row|, VP = P \ row(pivot), child
  *                        P' = P & row(q), EXPAND_R moves i in P' with |P' \ row(i)| == 1
  *                        into R when |P'| > 1)
- *   - .bin container:    src/graph.cc:206-265
+ *   - .bin container:    src/graph.cc:154-213
  *
  * The pivot tie rule here is canonical (lowest row index), which the GPU kernel
  * uses too, so node counts agree; the clique set does not depend on it.
@@ -173,7 +173,7 @@ static void finish_stats(og_graph *g) {
     if (d > md) md = (uint32_t)d;
   }
   g->max_degree = md;
-  g->degeneracy = md; /* the loader leaves degeneracy = max degree (src/graph.cc:201) */
+  g->degeneracy = md; /* the loader leaves degeneracy = max degree (src/graph.cc:149) */
 }
 
 og_graph *og_from_pairs(const uint32_t *u, const uint32_t *v, uint64_t npairs) {
@@ -189,7 +189,7 @@ og_graph *og_from_pairs(const uint32_t *u, const uint32_t *v, uint64_t npairs) {
   uint64_t m = 0;
   for (uint64_t i = 0; i < ne; i++)
     if (i == 0 || e[i] != e[i - 1]) e[m++] = e[i];
-  /* present labels, ascending (label_to_id, src/graph.cc:175-181) */
+  /* present labels, ascending (label_to_id, src/graph.cc:123-130) */
   uint64_t *lab = (uint64_t *)malloc((2 * m + 1) * sizeof(uint64_t));
   for (uint64_t i = 0; i < m; i++) { lab[2 * i] = e[i] >> 32; lab[2 * i + 1] = e[i] & 0xFFFFFFFFu; }
   radix_sort_u64(lab, 2 * m);
@@ -215,7 +215,7 @@ og_graph *og_from_pairs(const uint32_t *u, const uint32_t *v, uint64_t npairs) {
   uint64_t *fill = (uint64_t *)malloc((n + 1) * sizeof(uint64_t));
   memcpy(fill, g->off, (n + 1) * sizeof(uint64_t));
   /* edges in (u,v) order: each row receives its lower neighbours first, then
-   * its upper neighbours, both ascending -> rows come out sorted (graph.cc:187-197) */
+   * its upper neighbours, both ascending -> rows come out sorted (graph.cc:135-145) */
   for (uint64_t i = 0; i < m; i++) {
     g->adj[fill[eu[i]]++] = ev[i];
     g->adj[fill[ev[i]]++] = eu[i];
@@ -294,7 +294,7 @@ void og_sort_degeneracy(og_graph *g) {
   uint64_t len = 0;
   int64_t k = 0;
   /* level k: append every vertex whose residual degree is exactly k in id order,
-   * then cascade through the appended queue (graph.cc:341-356) */
+   * then cascade through the appended queue (graph.cc:289-304) */
   while (len < n) {
     uint64_t cur = len;
     k++;

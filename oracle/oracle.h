@@ -39,11 +39,11 @@ typedef struct og_result {
 uint64_t og_mix64(uint64_t x);
 uint64_t og_clique_hash(const uint32_t *labels, uint32_t size);
 
-/* Text COO parse with std::istream `>>` semantics (src/graph.cc:134-156). */
+/* Text COO parse with std::istream `>>` semantics (src/graph.cc:82-104). */
 int og_parse_text(const char *path, uint32_t **u, uint32_t **v, uint64_t *npairs);
 void og_free_buf(void *p);
 
-/* Graph construction with the reference loader conventions (src/graph.cc:116-204). */
+/* Graph construction with the reference loader conventions (src/graph.cc:64-152). */
 og_graph *og_from_pairs(const uint32_t *u, const uint32_t *v, uint64_t npairs);
 /* Graph from an already-built symmetric CSR with sorted rows (e.g. a GPU export). */
 og_graph *og_from_csr(uint32_t n, const uint64_t *off, const uint32_t *adj, const uint32_t *labels);
@@ -56,7 +56,7 @@ uint32_t og_degeneracy(const og_graph *g);
 /* Copies out CSR (off has n+1 entries, adj 2m) and labels; any pointer may be NULL. */
 void og_export(const og_graph *g, uint64_t *off, uint32_t *adj, uint32_t *labels);
 
-/* Degeneracy order exactly as Graph::SortByDegeneracy + ApplyOrder (src/graph.cc:333-358, 54-77). */
+/* Degeneracy order exactly as Graph::SortByDegeneracy + ApplyOrder (src/graph.cc:281-306, 54-77). */
 void og_sort_degeneracy(og_graph *g);
 /* Relabel with an explicit order: new id i is old vertex order[i]. */
 int og_apply_order(og_graph *g, const uint32_t *order);
@@ -84,7 +84,7 @@ int og_list_cliques(const og_graph *g, const char *path);
 void og_root_sizes(const og_graph *g, uint64_t begin, uint64_t end, uint32_t *p_out, uint32_t *x_out,
                    uint32_t *xc_out);
 
-/* The reference `.bin` container (src/graph.cc:206-265). */
+/* The reference `.bin` container (src/graph.cc:154-213). */
 int og_store_bin(const og_graph *g, const char *path);
 og_graph *og_load_bin(const char *path);
 

@@ -3,7 +3,7 @@
 TEST INFRASTRUCTURE ONLY: tests/, ``__graft_entry__.smoke()`` and bench.py's
 CPU-baseline leg import this module as the checker; the product package never
 does.  The C code it wraps restates the RDMCE reference's host loader
-(src/graph.cc), degeneracy order (src/graph.cc:333-358) and edge-rooted bitmap
+(src/graph.cc), degeneracy order (src/graph.cc:281-306) and edge-rooted bitmap
 Bron-Kerbosch with pivot (src/kernels/BkPivotBitBalance.cuh) on the CPU.
 """
 from __future__ import annotations

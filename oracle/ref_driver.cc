@@ -9,7 +9,7 @@
 //   ref_cpu pivot <graph>            MceSolver::Solve(BKPivot), 1 thread
 //   ref_cpu par <graph> <threads> [max_roots]
 //                                    root-parallel: one MceSolver per thread, the
-//                                    vertex roots of src/mce.cc:66-95 handed out in
+//                                    vertex roots of src/mce.cc:64-95 handed out in
 //                                    chunks, each solved by BKFixedMemPivotBit2
 //   ref_cpu steps <graph> <threads> <seconds> <warmup> <steps>
 //                                    bench steps: each step (a forked child)

@@ -2,7 +2,7 @@
 //
 // Replaces MceGpuSolver / BkSolverWrapper (src/mce_gpu.cu:9-22,
 // src/kernels/BkPivotBitBalance.cuh:611-678) and Graph's loaders
-// (src/graph.cc:116-265).  Every entry point returns a status; nothing exits.
+// (src/graph.cc:64-213).  Every entry point returns a status; nothing exits.
 #include <algorithm>
 #include <chrono>
 #include <cstring>

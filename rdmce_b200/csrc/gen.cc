@@ -6,7 +6,7 @@
 // planted cliques.  Every draw comes from a counter-based SplitMix64 stream, so
 // output is identical for any thread count.  Pairs are emitted raw: self-loops
 // and duplicates are left for the loader to drop, as the reference loader does
-// (src/graph.cc:140-163).
+// (src/graph.cc:88-111).
 #include <algorithm>
 #include <cmath>
 #include <cstring>

@@ -1,11 +1,11 @@
 // hostio.cc -- host-side graph file formats.
 //
-//  * COO text as Graph::LoadFromFile reads it (src/graph.cc:134-156): the file
+//  * COO text as Graph::LoadFromFile reads it (src/graph.cc:82-104): the file
 //    is a stream of unsigned decimal tokens; each record is `>> u >> v`
 //    (white space, newlines included, may separate the two), the rest of the
 //    line after v is ignored, and a failed extraction discards the rest of the
 //    current line.  '%' / '#' header lines therefore fall out as bad lines.
-//  * the reference .bin container (src/graph.cc:206-265): four native-endian
+//  * the reference .bin container (src/graph.cc:154-213): four native-endian
 //    size_t (n, m, max_degree, degeneracy), then per vertex a size_t degree and
 //    that many uint32 neighbours, then n uint32 original labels.
 #include <cerrno>

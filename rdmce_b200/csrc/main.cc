@@ -1,6 +1,6 @@
 // main.cc -- `RDMCE -i <graph> [-o a|d|deg|unchange] [-d id[,id..]] [-c]`
 //
-// The reference command line (main.cc:13-199): same options, same exit on a
+// The reference command line (main.cc:13-138): same options, same exit on a
 // bad option, and the same result lines ("MC numbers: N", "MCE GPU Time: t")
 // that scripts/analyze.sh parses.  Extra lines report the clique-size
 // histogram and the checksum.  `-d` with several ids splits the roots over

@@ -1,10 +1,10 @@
 // preprocess.cu -- COO pairs -> degeneracy-ordered CSR, entirely on the GPU.
 //
 // Replaces the reference's single-threaded host pipeline:
-//   Graph::LoadFromFile edge handling   src/graph.cc:140-204  (self-loops dropped,
+//   Graph::LoadFromFile edge handling   src/graph.cc:64-152  (self-loops dropped,
 //       u<v, sort+unique, dense relabel of present labels in ascending order)
-//   Graph::SortByDegeneracy/ApplyOrder  src/graph.cc:333-358, 54-77
-//   Graph::ConvertToCsr + LoadFromCpu   src/graph.cc:268-288, src/graph_gpu.cu:3-58
+//   Graph::SortByDegeneracy/ApplyOrder  src/graph.cc:281-306, 54-77
+//   Graph::ConvertToCsr + LoadFromCpu   src/graph.cc:216-236, src/graph_gpu.cu:3-58
 // Steps: pack (min,max) keys -> radix sort -> unique -> mark/scan dense ids ->
 // degrees -> k-core peeling in synchronous rounds (one cooperative launch) ->
 // relabel both edge directions -> radix sort -> CSR offsets by scan -> root
@@ -104,7 +104,7 @@ __global__ void k_iota(uint32_t *a, uint64_t n) {
 // residual degree fell to <= k, so x has at most k later neighbours -- a
 // degeneracy order.  The rounds make the order deterministic, so root ids
 // (edges of the ordered CSR) are stable from run to run; the reference's
-// sequential queue (graph.cc:341-356) orders vertices inside a round
+// sequential queue (graph.cc:289-304) orders vertices inside a round
 // differently, which changes neither the degeneracy nor the clique set.
 struct PeelCtl {
   uint32_t fcnt[3];     // frontier sizes, by round mod 3
@@ -516,7 +516,7 @@ mce_status build_from_pairs(const uint32_t *u, const uint32_t *v, uint64_t np, i
   flags.release();
   pos.release();
 
-  // 2) dense ids of present labels, ascending (src/graph.cc:175-181)
+  // 2) dense ids of present labels, ascending (src/graph.cc:123-130)
   const uint64_t nl = (uint64_t)maxlab + 1;
   DevBuf<uint32_t> mark, id;
   MCE_TRY(mark.alloc(nl + 1, st));
@@ -560,7 +560,7 @@ mce_status finish_graph(uint32_t n, uint64_t m, const uint32_t *eu, const uint32
   DevBuf<uint32_t> order, rank;
   MCE_TRY(order.alloc(n, st));
   MCE_TRY(rank.alloc(n, st));
-  g->degeneracy = g->max_degree;  // Graph::LoadFromFile leaves degeneracy_ = max degree (graph.cc:201)
+  g->degeneracy = g->max_degree;  // Graph::LoadFromFile leaves degeneracy_ = max degree (graph.cc:149)
   if (order_kind == MCE_ORDER_DEGENERACY && n > 0) {
     DevBuf<uint32_t> off0, cursor, adj0;
     MCE_TRY(off0.alloc(n + 1, st));

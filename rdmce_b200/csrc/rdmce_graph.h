@@ -34,14 +34,14 @@ class Graph {
   Graph(Graph &&other) noexcept;
   ~Graph();
 
-  // COO text, src/graph.cc:116-204 (the edge list is kept on the host until
+  // COO text, src/graph.cc:64-152 (the edge list is kept on the host until
   // SortByOrder / the first solve builds the device graph)
   void LoadFromFile(const std::string &path);
-  // the reference .bin container, already ordered (src/graph.cc:230-265)
+  // the reference .bin container, already ordered (src/graph.cc:178-213)
   void LoadFromBin(const std::string &path);
-  // writes <path without extension>.bin, as src/graph.cc:206-228 does
+  // writes <path without extension>.bin, as src/graph.cc:154-176 does
   void StoreIntoBin(const std::string &path);
-  // fills the host CSR returned by GetRowOffset / GetColIdx (src/graph.cc:268-288)
+  // fills the host CSR returned by GetRowOffset / GetColIdx (src/graph.cc:216-236)
   void ConvertToCsr();
   void SortByOrder(OrderType order);
 

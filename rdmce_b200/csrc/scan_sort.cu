@@ -2,7 +2,7 @@
 // 64-bit keys and max-reduction, plus the per-device scratch cache.
 //
 // These replace the host-side std::sort / std::unique / prefix loops of the
-// reference loader (src/graph.cc:161-197, 268-288) with HBM-bound passes.
+// reference loader (src/graph.cc:109-145, 216-236) with HBM-bound passes.
 // Radix sort: 8-bit digits; per pass one histogram kernel (tile = 4096 keys),
 // one scan over the digit-major (digit, tile) counts, and one stable scatter
 // that ranks keys with __match_any_sync, reorders the tile in shared memory and

@@ -4,7 +4,7 @@ Each fixture is a small edge list plus the expected clique count, clique-size
 histogram and checksum.  Expected values come from networkx.find_cliques (an
 independent Bron-Kerbosch implementation), restricted to the vertices that
 appear in at least one non-loop edge -- the reference loader drops the others
-(RDMCE src/graph.cc:140-181).  The checksum is the engine's order-independent
+(RDMCE src/graph.cc:64-152).  The checksum is the engine's order-independent
 set hash: sum over cliques C (mod 2^64) of
 mix64(s1 ^ rotl(s2, 31) ^ (|C| << 56)), s1 = sum mix64(l), s2 = sum
 mix64(l ^ 0x9E3779B97F4A7C15) over the labels l of C, mix64 = SplitMix64's
