@@ -121,6 +121,34 @@ uint64_t mce_launch_count(void);
  * in word-ops per second: the integer-pipe roof of the enumeration kernel. */
 mce_status mce_probe_int_peak(int device, double *word_ops_per_s);
 
+/* Allocation-free CSR row offsets.  No counterpart in the reference, which
+ * builds offsets on the host (Graph::ConvertToCsr, src/graph.cc:216-236).
+ * Both arrays are in device memory: rowoffset_device[i] = degree_device[0] +
+ * ... + degree_device[i-1] for i = 0..n (n + 1 entries; the last one is the
+ * total; sums are taken mod 2^32).  The engine's graph builders run the same
+ * three-pass scan with a partial-sum buffer they allocate on every call; this
+ * variant keeps the partial sums in a fixed 129 KiB array compiled into the
+ * library and allocates nothing, on the device or the host.  It is meant for
+ * callers that cannot allocate at the point of the call: a serving loop that
+ * has handed all free HBM to resident graphs (cudaMalloc would fail), or code
+ * whose caching allocator holds the device's whole pool, or any loop where an
+ * allocation's implicit device synchronisation would stall other streams.
+ *   - n > MCE_STATIC_SCAN_MAX_N (2^26 degrees) returns MCE_ERR_TOO_LARGE
+ *     before anything is enqueued.
+ *   - The first call on each device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current and caches it; make
+ *     that first call before any stream capture begins on the device.
+ *   - Nothing has to be zeroed first: every partial sum is written before it
+ *     is read, and all n + 1 offsets are written.
+ *   - One array serves every caller on a device: calls that overlap in time
+ *     on one device (from any stream or thread) race and corrupt each other's
+ *     results.  Serialise them, e.g. by issuing them on one stream.
+ *   - The work is enqueued on `stream` (a cudaStream_t, NULL = the legacy
+ *     default stream); the call returns without waiting for it. */
+#define MCE_STATIC_SCAN_MAX_N 67108864ull
+mce_status mce_csr_offsets_static(int device, const uint32_t *degree_device, uint32_t *rowoffset_device,
+                                  uint64_t n, void *stream);
+
 /* COO pairs in host memory -> device-resident, degeneracy-ordered CSR.
  * Replaces Graph::LoadFromFile's edge handling + SortByOrder + ConvertToCsr +
  * GraphGpu::LoadFromCpu (src/graph.cc:64-152, 281-306, 216-236;

@@ -155,6 +155,7 @@ _SIGS = {
     "mce_solve_roots": (_I, [_P, _P, _U64, C.POINTER(Options), _P, _P]),
     "mce_solve_root_list": (_I, [_P, _P, _U64, C.POINTER(Options), C.POINTER(_Result)]),
     "mce_launch_count": (_U64, []),
+    "mce_csr_offsets_static": (_I, [_I, _P, _P, _U64, _P]),
     "mce_probe_int_peak": (_I, [_I, C.POINTER(_D)]),
     "mce_solve_coo": (_I, [_P, _P, _U64, C.POINTER(Options), C.POINTER(_Result)]),
     "mce_batch_create": (_I, [_P, _P, _P, _U32, C.POINTER(Options), C.POINTER(_P)]),

@@ -113,6 +113,15 @@ mce_status mce_probe_int_peak(int device, double *word_ops_per_s) {
   return probe_int_peak(device, word_ops_per_s);
 }
 
+mce_status mce_csr_offsets_static(int device, const uint32_t *degree_device, uint32_t *rowoffset_device,
+                                  uint64_t n, void *stream) {
+  // size check first: an oversized request returns before touching the device
+  if (n > MCE_STATIC_SCAN_MAX_N) return MCE_ERR_TOO_LARGE;
+  if (!rowoffset_device || (n && !degree_device)) return MCE_ERR_INVALID_ARG;
+  MCE_TRY(set_device(device));
+  return csr_offsets_static(device, degree_device, rowoffset_device, n, (cudaStream_t)stream);
+}
+
 void mce_default_options(mce_options *opt) {
   if (opt) *opt = defaults();
 }

@@ -107,6 +107,9 @@ mce_status scan_exclusive_u64(const uint64_t *in, uint64_t *out, uint64_t n, uin
                               cudaStream_t st);
 // LSD radix sort of n 64-bit keys over bits [0, bits); result in *keys (tmp = scratch of n)
 mce_status radix_sort_u64(uint64_t *keys, uint64_t *tmp, uint64_t n, int bits, cudaStream_t st);
+// allocation-free CSR offsets: off[0..n] = exclusive scan of deg, off[n] = total;
+// partial sums in a fixed device array (n <= 2^26); calls on one device must not overlap
+mce_status csr_offsets_static(int device, const uint32_t *deg, uint32_t *off, uint64_t n, cudaStream_t st);
 // reduce max of n uint32
 mce_status reduce_max_u32(const uint32_t *in, uint64_t n, uint32_t *d_out, cudaStream_t st);
 

@@ -235,6 +235,67 @@ mce_status scan_exclusive_u64(const uint64_t *in, uint64_t *out, uint64_t n, uin
   return scan_impl<uint64_t>(in, out, n, d_total, st);
 }
 
+// ---- allocation-free exclusive scan (mce_csr_offsets_static) ----
+// The partial sums of the three-pass scan live in this fixed array instead of
+// a buffer allocated per call: level 1 holds one sum per 2048-element tile of
+// the input (at most kStaticScanMaxN / 2048 = 32768), level 2 one sum per tile
+// of level 1 (at most 16).  Every entry is written before it is read, so
+// nothing in it has to start at zero.  All callers on a device share it:
+// calls that overlap in time on one device race.
+constexpr uint64_t kStaticScanMaxN = 1ULL << 26;
+constexpr uint64_t kStaticL1 = kStaticScanMaxN / kScanTile;
+constexpr uint64_t kStaticL2 = kStaticL1 / kScanTile;
+static_assert(kStaticL1 == 32768 && kStaticL2 == 16, "static scan layout");
+static __device__ __align__(256) uint32_t g_static_scan_sums[kStaticL1 + 256];
+
+namespace {
+std::mutex g_static_scan_mu;
+uint32_t *g_static_scan_addr[64];  // device address of g_static_scan_sums, per device
+}  // namespace
+
+mce_status csr_offsets_static(int device, const uint32_t *deg, uint32_t *off, uint64_t n, cudaStream_t st) {
+  if (n > kStaticScanMaxN) return MCE_ERR_TOO_LARGE;
+  if (!off || (n && !deg) || device < 0 || device >= 64) return MCE_ERR_INVALID_ARG;
+  uint32_t *sums = nullptr;
+  {
+    // first call on this device: look the array up with the device current
+    std::lock_guard<std::mutex> lk(g_static_scan_mu);
+    if (!g_static_scan_addr[device]) {
+      void *p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scan_sums);
+      if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        return cuda_status(e == cudaSuccess ? cudaErrorInvalidSymbol : e);
+      }
+      g_static_scan_addr[device] = (uint32_t *)p;
+    }
+    sums = g_static_scan_addr[device];
+  }
+  if (n == 0) {
+    MCE_CUDA_TRY(cudaMemsetAsync(off, 0, sizeof(uint32_t), st));
+    return MCE_OK;
+  }
+  const uint64_t tiles = (n + kScanTile - 1) / kScanTile;
+  if (tiles == 1) {
+    k_tile_scan<uint32_t><<<1, kScanThreads, 0, st>>>(deg, off, n, nullptr, off + n); note_launch();
+    MCE_CUDA_TRY(cudaGetLastError());
+    return MCE_OK;
+  }
+  uint32_t *l1 = sums, *l2 = sums + kStaticL1;
+  k_tile_sums<uint32_t><<<(unsigned)tiles, kScanThreads, 0, st>>>(deg, n, l1); note_launch();
+  const uint64_t tiles2 = (tiles + kScanTile - 1) / kScanTile;
+  if (tiles2 == 1) {
+    k_tile_scan<uint32_t><<<1, kScanThreads, 0, st>>>(l1, l1, tiles, nullptr, nullptr); note_launch();
+  } else {
+    k_tile_sums<uint32_t><<<(unsigned)tiles2, kScanThreads, 0, st>>>(l1, tiles, l2); note_launch();
+    k_tile_scan<uint32_t><<<1, kScanThreads, 0, st>>>(l2, l2, tiles2, nullptr, nullptr); note_launch();
+    k_tile_scan<uint32_t><<<(unsigned)tiles2, kScanThreads, 0, st>>>(l1, l1, tiles, l2, nullptr); note_launch();
+  }
+  k_tile_scan<uint32_t><<<(unsigned)tiles, kScanThreads, 0, st>>>(deg, off, n, l1, off + n); note_launch();
+  MCE_CUDA_TRY(cudaGetLastError());
+  return MCE_OK;
+}
+
 mce_status radix_sort_u64(uint64_t *keys, uint64_t *tmp, uint64_t n, int bits, cudaStream_t st) {
   if (n < 2 || bits <= 0) return MCE_OK;
   uint64_t ntiles64 = (n + kSortTile - 1) / kSortTile;
