@@ -20,7 +20,8 @@ from dataclasses import dataclass, field
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "librdmce.so")
+# RDMCE_LIB points the binding at another build of the same library
+LIB_PATH = os.environ.get("RDMCE_LIB", os.path.join(HERE, "librdmce.so"))
 CLI_PATH = os.path.join(HERE, "bin", "RDMCE")
 HIST_LEN = 8192
 PHASES = 6
@@ -52,7 +53,8 @@ class Options(C.Structure):
         ("spin_limit", C.c_uint64),
         ("stream", C.c_void_p),
         ("flags", C.c_uint32),
-        ("reserved", C.c_uint32 * 7),
+        ("reg_share_bound", C.c_uint32),
+        ("reserved", C.c_uint32 * 6),
     ]
 
 

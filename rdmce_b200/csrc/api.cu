@@ -325,6 +325,7 @@ static mce_status solve_impl(mce_graph *g, const mce_options &o, mce_result *out
   cfg.warps_per_block = o.warps_per_block;
   cfg.blocks_per_sm = o.blocks_per_sm;
   cfg.share_bound = o.share_bound ? o.share_bound : 24;
+  cfg.reg_share_bound = o.reg_share_bound;
   cfg.expand_r = o.expand_r;
   cfg.sharing = (o.flags & MCE_FLAG_NO_SHARING) ? 0 : 1;
   cfg.root_begin = o.root_begin;

@@ -43,6 +43,7 @@ struct EnumConfig {
   uint32_t warps_per_block = 0;
   uint32_t blocks_per_sm = 0;
   uint32_t share_bound = 24;
+  uint32_t reg_share_bound = 0;  // 0 = default
   int expand_r = 1;
   int sharing = 1;
   uint64_t root_begin = 0, root_end = 0;
@@ -98,7 +99,8 @@ struct EnumParams {
   unsigned long long *per_root_checksum;
   int expand_r;
   int sharing;                           // root-down exposure through the task pool
-  uint32_t share_bound;                  // expose only levels with |P| >= this
+  uint32_t share_bound;                  // expose only levels with |P| >= this (general tier)
+  uint32_t reg_share_bound;              // the same inside the register tiers
   uint32_t nwarps;
   uint64_t spin_limit;                   // bound on every device-side wait
   unsigned int *error;

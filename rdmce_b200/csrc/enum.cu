@@ -54,6 +54,10 @@ constexpr uint32_t kT1Depth = 66;         // 64-bit tier: levels (<= 64 columns 
 constexpr uint32_t kT0Depth = 34;         // 32-bit tier: levels (<= 32 columns + root)
 constexpr uint32_t kHdr = 64;             // task record header bytes
 constexpr uint32_t kLocalRec = 2048;      // per-warp local task record (64-bit-tier size)
+// Default tau inside the register tiers.  Their levels have at most 64 (T1)
+// or 32 (T0) candidates, so the general tier's tau of 24 would leave most of
+// their subtrees unshareable.
+constexpr uint32_t kRegShareBound = 12;
 // phases of the per-warp cycle accounting
 enum { kCycBuild = 0, kCycReg = 1, kCycGen = 2, kCycSpawn = 3, kCycIdle = 4, kCycQueue = 5, kCycPhases = 6 };
 
@@ -75,6 +79,17 @@ __host__ __device__ __forceinline__ uint64_t task_bytes(uint32_t pc, uint32_t nr
   return kHdr + align8(4ULL * pc) + 8ULL * nrows * W;
 }
 
+// A general-tier subproblem laid out in the warp's slab.
+struct Gen {
+  const uint64_t *rows;
+  const uint32_t *colv;
+  const uint64_t *h1s, *h2s;
+  uint64_t *stack;
+  uint32_t *alist;
+  uint64_t alist_cap;
+  uint32_t pc, nrows, W;
+};
+
 // Per-warp shared memory.  All mutable per-warp state outside the tier loops
 // lives here (lane 0 updates the scalars), so the small Ctx handle can be
 // passed by value.
@@ -95,7 +110,19 @@ struct WarpSmem {
   unsigned long long count, checksum, nodes, wops;
   uint32_t max_size, slot, pending, pad;
   unsigned long long cyc[kCycPhases];  // clock64 cycles by phase
+  // The tiers enclosing the running subproblem.  A nested tier exposes their
+  // open levels (shallower, so larger) before its own: rows and column ids of
+  // the running 64-bit-tier solve, the running general-tier solve, and the
+  // level each of them is expanding.
+  uint64_t t1rows[kT1Rows];
+  uint32_t t1cv[64];
+  Gen gen;
+  int t1_level, gen_level;
+  uint32_t t1_pc;
+  uint32_t nest;  // bit 0: a general-tier solve is running; bit 1: a 64-bit-tier solve
 };
+
+constexpr uint32_t kNestGen = 1, kNestT1 = 2;
 
 struct Ctx {
   const EnumParams *P;
@@ -194,7 +221,7 @@ __device__ bool ring_push(uint32_t *slots, unsigned long long *seq, unsigned lon
 
 __device__ bool ring_pop(uint32_t *slots, unsigned long long *seq, unsigned long long *head,
                          unsigned long long *tail, uint32_t mask, uint32_t *val, const EnumParams &P) {
-  for (int tries = 0; tries < 32; tries++) {
+  for (int tries = 0; tries < 8; tries++) {
     const unsigned long long h = *(volatile unsigned long long *)head;
     const unsigned long long t = *(volatile unsigned long long *)tail;
     if (h >= t) return false;
@@ -328,6 +355,15 @@ __device__ __forceinline__ void compress_row(const uint64_t *row, const uint64_t
   if (cb) out[wi] = cur;
 }
 
+// Expose open levels of the enclosing general-tier / 64-bit-tier solve, if one
+// is running; true if anything was exposed.  Defined after those tiers.
+__device__ __noinline__ bool spawn_outer_gen(Ctx c);
+__device__ __noinline__ bool spawn_outer_t1(Ctx c);
+// Exposure from inside the 32-bit tier: enclosing tiers first, then its own
+// levels.  One out-of-line call keeps the node loop's registers free.
+struct T0;
+__device__ __noinline__ void t0_share(Ctx c, const T0 t, int level);
+
 // ---------------------------------------------------------- 32-bit tier
 // At most 32 candidate columns and 32 rows: lane l holds row l as a 32-bit
 // word (rows 0..pc-1 are the column vertices, the rest X rows) plus the label
@@ -380,7 +416,7 @@ __device__ void t0_spawn(const Ctx &c, const T0 &t, int level) {
   for (; l < level; l++) {
     const uint4 f = sm->t0f[l];
     open = f.x & f.y;
-    if (open && (uint32_t)__popc(f.x) + 1 >= c.P->share_bound) break;
+    if (open && (uint32_t)__popc(f.x) + 1 >= c.P->reg_share_bound) break;
     open = 0;
   }
   if (!open) return;
@@ -470,11 +506,7 @@ __device__ __noinline__ void t0_solve_body(Ctx c, T0 t, uint32_t pc, uint32_t nr
       fresh = true;
       if (c.sharing && ++tick >= 128) {
         tick = 0;
-        if (hungry(c)) {
-          const unsigned long long t0 = now();
-          t0_spawn(c, t, level);
-          if (lane == 0) sm->cyc[kCycSpawn] += now() - t0;
-        }
+        if (hungry(c)) t0_share(c, t, level);
       }
       continue;
     }
@@ -614,16 +646,16 @@ __device__ void t1_materialize(const Ctx &c, const T1 &t, uint64_t Pbase, uint32
   __syncwarp();
 }
 
-__device__ void t1_spawn(const Ctx &c, const T1 &t, int level) {
+__device__ bool t1_spawn(const Ctx &c, const T1 &t, int level) {
   WarpSmem *sm = c.sm;
   int l = 0;
   uint64_t open = 0;
   for (; l < level; l++) {
     open = sm->fP[l] & sm->fVP[l];
-    if (open && (uint32_t)__popcll(sm->fP[l]) + 1 >= c.P->share_bound) break;
+    if (open && (uint32_t)__popcll(sm->fP[l]) + 1 >= c.P->reg_share_bound) break;
     open = 0;
   }
-  if (!open) return;
+  if (!open) return false;
   const uint64_t Pl = sm->fP[l];
   uint64_t VPl = sm->fVP[l];
   const uint32_t abl = sm->fab[l][c.lane];
@@ -642,6 +674,7 @@ __device__ void t1_spawn(const Ctx &c, const T1 &t, int level) {
   }
   if (c.lane == 0) sm->fVP[l] = VPl;
   __syncwarp();
+  return true;
 }
 
 __device__ __noinline__ void t1_solve_body(Ctx c, T1 t, uint32_t pc, uint32_t nrows, uint32_t rsize0, uint64_t s10,
@@ -656,6 +689,15 @@ __device__ __noinline__ void t1_solve_body(Ctx c, T1 t, uint32_t pc, uint32_t nr
   uint64_t P = pc >= 64 ? ~0ULL : ((1ULL << pc) - 1);
   uint64_t VP = 0;
   uint32_t rsize = rsize0;
+#pragma unroll
+  for (int j = 0; j < kRPL; j++) sm->t1rows[32 * j + lane] = t.r[j];
+  sm->t1cv[lane] = t.cva;
+  sm->t1cv[lane + 32] = t.cvb;
+  if (lane == 0) {
+    sm->t1_pc = pc;
+    sm->nest |= kNestT1;
+  }
+  __syncwarp();
   uint64_t s1 = s10, s2 = s20;
   unsigned long long nodes = 0, wops = 0;  // nodes uniform; wops per lane
   int level = 0;
@@ -747,8 +789,22 @@ __device__ __noinline__ void t1_solve_body(Ctx c, T1 t, uint32_t pc, uint32_t nr
         t0.cv = lane < pc2 ? sm->xcv[lane] : 0;
         t0.h1 = lane < pc2 ? sm->xh1[lane] : 0;
         t0.h2 = lane < pc2 ? sm->xh2[lane] : 0;
+        if (lane == 0) sm->t1_level = level;
         __syncwarp();
         t0_solve_body(c, t0, pc2, nact, rs, n1, n2);
+        // the child may have exposed open candidates of this level
+        VP = sm->fVP[level];
+        // While the child ran, the levels above it were exposed only through
+        // the child's own checks; offer them here as well.
+        if (c.sharing && ++tick >= 4) {
+          tick = 0;
+          if (hungry(c)) {
+            const unsigned long long ts = now();
+            if (!spawn_outer_gen(c)) t1_spawn(c, t, level + 1);
+            if (lane == 0) sm->cyc[kCycSpawn] += now() - ts;
+            VP = sm->fVP[level];
+          }
+        }
         continue;  // next candidate at this level
       }
       level++;
@@ -763,7 +819,7 @@ __device__ __noinline__ void t1_solve_body(Ctx c, T1 t, uint32_t pc, uint32_t nr
         tick = 0;
         if (hungry(c)) {
           const unsigned long long t0 = now();
-          t1_spawn(c, t, level);
+          if (!spawn_outer_gen(c)) t1_spawn(c, t, level);
           if (lane == 0) sm->cyc[kCycSpawn] += now() - t0;
         }
       }
@@ -784,6 +840,7 @@ __device__ __noinline__ void t1_solve_body(Ctx c, T1 t, uint32_t pc, uint32_t nr
   if (lane == 0) {
     sm->nodes += nodes;
     sm->wops += wops;
+    sm->nest &= ~kNestT1;
   }
   __syncwarp();
   maybe_flush(c);
@@ -816,16 +873,6 @@ __device__ void reg_from_local(const Ctx &c, const char *rec) {
 
 // --------------------------------------------------------- general tier
 
-struct Gen {
-  const uint64_t *rows;
-  const uint32_t *colv;
-  const uint64_t *h1s, *h2s;
-  uint64_t *stack;
-  uint32_t *alist;
-  uint64_t alist_cap;
-  uint32_t pc, nrows, W;
-};
-
 // Child of candidate q at a general-tier level (record rec_l) as a task
 // record in `out`: columns = Pbase & row(q), rows = active rows holding bit q
 // (and all of R' when the level's list is inherited), compressed to the child
@@ -833,6 +880,7 @@ struct Gen {
 __device__ bool gen_materialize(const Ctx &c, const Gen &G, const uint64_t *rec_l, uint32_t q,
                                 const uint64_t *Pbase, uint64_t max_bytes, char *out) {
   const uint32_t lane = c.lane, W = G.W;
+  if (W > 64) return false;  // the child's column mask lives in rowbuf (64 words)
   uint64_t *CP = c.sm->rowbuf;
   const uint64_t *rowq = G.rows + (uint64_t)q * W;
   uint32_t pc = 0;
@@ -910,7 +958,7 @@ __device__ bool gen_materialize(const Ctx &c, const Gen &G, const uint64_t *rec_
   return true;
 }
 
-__device__ void gen_spawn(const Ctx &c, const Gen &G, int level) {
+__device__ bool gen_spawn(const Ctx &c, const Gen &G, int level) {
   const uint32_t W = G.W, lane = c.lane;
   const uint64_t LREC = 3ULL * W + 4;
   int l = -1;
@@ -925,7 +973,7 @@ __device__ void gen_spawn(const Ctx &c, const Gen &G, int level) {
     pc = __reduce_add_sync(kFull, pc);
     if (__any_sync(kFull, any) && pc + 1 >= c.P->share_bound) l = k;
   }
-  if (l < 0) return;
+  if (l < 0) return false;
   uint64_t *rec = G.stack + (uint64_t)l * LREC;
   uint64_t *Pl = rec, *VPl = rec + W;
   // scratch record past the deepest level holds Pbase
@@ -938,7 +986,7 @@ __device__ void gen_spawn(const Ctx &c, const Gen &G, int level) {
       if (!open) break;
       const uint32_t q = wq * 64 + (63 - __clzll((long long)open));
       uint32_t blk;
-      if (!pool_alloc(c, &blk)) return;
+      if (!pool_alloc(c, &blk)) return spawned > 0;
       for (uint32_t w = lane; w < W; w += 32) {
         const uint64_t below = (int)w < wq ? ~0ULL : ((int)w == wq ? ((1ULL << (q & 63)) - 1) : 0);
         Pbase[w] = Pl[w] & ~(VPl[w] & below);
@@ -947,7 +995,7 @@ __device__ void gen_spawn(const Ctx &c, const Gen &G, int level) {
       const bool ok = gen_materialize(c, G, rec, q, Pbase, c.P->block_bytes, pool_block(*c.P, blk));
       if (!ok) {
         pool_free(c, blk);
-        return;
+        return spawned > 0;
       }
       pool_publish(c, blk);
       if (lane == 0) VPl[wq] &= ~(1ULL << (q & 63));
@@ -955,6 +1003,7 @@ __device__ void gen_spawn(const Ctx &c, const Gen &G, int level) {
       spawned++;
     }
   }
+  return spawned > 0;
 }
 
 // Solve a general-tier ego network laid out in the slab.
@@ -967,6 +1016,10 @@ __device__ __noinline__ void gen_solve_body(Ctx c, Gen G, uint32_t rsize0, uint6
   const uint64_t *rows = G.rows;
   char *local = c.slab + c.slab_bytes - kLocalRec;
   unsigned long long nodes = 0, wops = 0;
+  if (lane == 0) {
+    sm->gen = G;
+    sm->nest |= kNestGen;
+  }
   for (uint32_t w = lane; w < W; w += 32) {
     const uint32_t lo = w * 64;
     stack[w] = (G.pc - lo >= 64) ? ~0ULL : ((1ULL << (G.pc - lo)) - 1);
@@ -1107,6 +1160,8 @@ __device__ __noinline__ void gen_solve_body(Ctx c, Gen G, uint32_t rsize0, uint6
         ccount += __popc(__ballot_sync(kFull, keep));
       }
       if (ccount <= kT1Rows && gen_materialize(c, G, rec, q, Pv, kLocalRec, local)) {
+        if (lane == 0) sm->gen_level = level;
+        __syncwarp();
         const unsigned long long t0 = now(), sp0 = sm->cyc[kCycSpawn];
         reg_from_local(c, local);
         // the register-tier time is booked there; keep it out of this phase
@@ -1218,9 +1273,34 @@ __device__ __noinline__ void gen_solve_body(Ctx c, Gen G, uint32_t rsize0, uint6
   if (lane == 0) {
     sm->nodes += nodes;
     sm->wops += wops;
+    sm->nest &= ~kNestGen;
   }
   __syncwarp();
   maybe_flush(c);
+}
+
+__device__ __noinline__ bool spawn_outer_gen(Ctx c) {
+  if (!(c.sm->nest & kNestGen)) return false;
+  const Gen G = c.sm->gen;
+  return gen_spawn(c, G, c.sm->gen_level + 1);
+}
+
+__device__ __noinline__ bool spawn_outer_t1(Ctx c) {
+  WarpSmem *sm = c.sm;
+  if (!(sm->nest & kNestT1)) return false;
+  T1 t;
+#pragma unroll
+  for (int j = 0; j < kRPL; j++) t.r[j] = sm->t1rows[32 * j + c.lane];
+  t.cva = sm->t1cv[c.lane];
+  t.cvb = sm->t1cv[c.lane + 32];
+  t1_hashes(c, t, sm->t1_pc);
+  return t1_spawn(c, t, sm->t1_level + 1);
+}
+
+__device__ __noinline__ void t0_share(Ctx c, const T0 t, int level) {
+  const unsigned long long ts = now();
+  if (!spawn_outer_gen(c) && !spawn_outer_t1(c)) t0_spawn(c, t, level);
+  if (c.lane == 0) c.sm->cyc[kCycSpawn] += now() - ts;
 }
 
 __device__ __forceinline__ void gen_solve(const Ctx &c, const Gen &G, uint32_t rsize0, uint64_t s10, uint64_t s20) {
@@ -1485,8 +1565,12 @@ __global__ void __launch_bounds__(256, 2) k_enumerate(const __grid_constant__ En
   if (c.lane == 0) {
     sm->count = sm->checksum = sm->nodes = sm->wops = 0;
     sm->max_size = sm->slot = sm->pending = 0;
+    sm->nest = 0;
     for (int i = 0; i < kCycPhases; i++) sm->cyc[i] = 0;
   }
+  __shared__ unsigned int s_poll;  // the block's poll token (see the idle loop)
+  if (threadIdx.x == 0) s_poll = 0;
+  __syncthreads();
   const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   c.slab = P.slab + gwarp * P.slab_bytes;
   c.slab_bytes = P.slab_bytes;
@@ -1496,6 +1580,7 @@ __global__ void __launch_bounds__(256, 2) k_enumerate(const __grid_constant__ En
   unsigned long long nroots = 0;
   bool roots_left = true;
   uint64_t idle_spins = 0;
+  uint32_t quiet = 0;  // consecutive "nobody busy, queue empty" observations
   // a warp counts itself busy from its first root claim until a claim fails,
   // so warps that start late (not co-resident) are never waited for
   if (c.lane == 0) atomicAdd(P.active, 1u);
@@ -1548,31 +1633,49 @@ __global__ void __launch_bounds__(256, 2) k_enumerate(const __grid_constant__ En
       if (c.lane == 0) atomicSub(P.active, 1u);
       if (!c.sharing) break;
     }
-    // Idle.  Read the busy count before the queue: a task is published before
-    // its producer stops counting as busy, so "nobody busy" followed by "queue
-    // empty" means no work can appear any more.  An idle warp counts itself
-    // busy only when it sees a queued task, and before it takes it.
+    // Idle.  At most one warp per block polls the global queue at a time (the
+    // block's poll token); the others sleep.  A warp counts itself busy only
+    // after it has taken a task, so a failed attempt costs no atomic on the
+    // busy count.  Reading the busy count before the queue: a task is
+    // published before its producer stops counting as busy, so "nobody busy"
+    // then "queue empty" means no work is left -- except for a task taken
+    // between the two reads, whose taker then finishes everything it exposes
+    // by itself if all others have left.  Exit waits for two such
+    // observations a back-off apart, which makes that case rare.
     bool done = false, got = false;
     uint32_t b = 0;
     const unsigned long long ti0 = now();
     if (c.lane == 0) {
-      const uint32_t act = *(volatile unsigned int *)P.active;
-      __threadfence();
-      const unsigned long long rh = *(volatile unsigned long long *)P.ready_head;
-      const unsigned long long rt = *(volatile unsigned long long *)P.ready_tail;
-      if (rh < rt) {
-        atomicAdd(P.active, 1u);
-        got = ring_pop(P.ready_slot, P.ready_seq, P.ready_head, P.ready_tail, P.pool_mask, &b, P);
-        if (!got) atomicSub(P.active, 1u);
-      } else if (act == 0) {
-        done = true;
-      } else if (++idle_spins > P.spin_limit) {
-        atomicExch(P.error, 1u);
-        done = true;
-      } else {
-        // back off, with jitter, so idle warps do not hammer the control words
-        const uint32_t shift = idle_spins < 6 ? (uint32_t)idle_spins : 6u;
-        __nanosleep((256u << shift) + ((uint32_t)(clock64() >> 3) & 1023u));
+      bool polled = false, seen = false;
+      if (atomicCAS(&s_poll, 0u, 1u) == 0u) {
+        polled = true;
+        const uint32_t act = *(volatile unsigned int *)P.active;
+        __threadfence();
+        const unsigned long long rh = *(volatile unsigned long long *)P.ready_head;
+        const unsigned long long rt = *(volatile unsigned long long *)P.ready_tail;
+        if (rh < rt) {
+          seen = true;
+          got = ring_pop(P.ready_slot, P.ready_seq, P.ready_head, P.ready_tail, P.pool_mask, &b, P);
+          if (got) atomicAdd(P.active, 1u);
+          quiet = 0;
+        } else if (act == 0) {
+          if (++quiet >= 2) done = true;
+        } else {
+          quiet = 0;
+        }
+        atomicExch(&s_poll, 0u);
+      }
+      if (!got && !done) {
+        if (++idle_spins > P.spin_limit) {
+          atomicExch(P.error, 1u);
+          done = true;
+        } else if (!polled || seen) {
+          __nanosleep(500u + ((uint32_t)(clock64() >> 3) & 511u));
+        } else {
+          // back off, with jitter, so idle warps do not hammer the control words
+          const uint32_t shift = idle_spins < 6 ? (uint32_t)idle_spins : 6u;
+          __nanosleep((256u << shift) + ((uint32_t)(clock64() >> 3) & 1023u));
+        }
       }
       sm->cyc[kCycIdle] += now() - ti0;
     }
@@ -1581,6 +1684,7 @@ __global__ void __launch_bounds__(256, 2) k_enumerate(const __grid_constant__ En
       solve_block(c, __shfl_sync(kFull, b, 0));
       if (c.lane == 0) atomicSub(P.active, 1u);
       idle_spins = 0;
+      quiet = 0;
       continue;
     }
     if (__shfl_sync(kFull, done, 0)) break;
@@ -1679,6 +1783,7 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
   P.spin_limit = cfg.spin_limit ? cfg.spin_limit : (1ULL << 34);
   P.sharing = (cfg.sharing && cfg.per_root_count == nullptr) ? 1 : 0;
   P.share_bound = cfg.share_bound ? cfg.share_bound : 24;
+  P.reg_share_bound = std::min(P.share_bound, cfg.reg_share_bound ? cfg.reg_share_bound : kRegShareBound);
   mce_status s = MCE_OK;
   EnumCtl *ctl = (EnumCtl *)scr->get(1, sizeof(EnumCtl), &s);
   if (!ctl) return s;
