@@ -80,6 +80,7 @@ typedef struct mce_options {
 #define MCE_FLAG_NO_SHARING 1u   /* disable inter-warp task sharing (the NB ablation) */
 #define MCE_FLAG_PER_ROOT   2u   /* fill per-root counts (mce_solve_roots) */
 #define MCE_FLAG_QUIET      4u
+#define MCE_FLAG_STATS      8u   /* count search-tree nodes and word-ops into mce_result (slower) */
 
 typedef struct mce_result {
   uint64_t count;             /* maximal cliques */
@@ -93,8 +94,8 @@ typedef struct mce_result {
   uint64_t roots;             /* roots enumerated */
   uint64_t shared_tasks;      /* tasks handed between warps */
   uint64_t heavy_roots;       /* roots that went through the large-scratch pass */
-  uint64_t nodes;             /* search-tree nodes visited */
-  uint64_t word_ops;          /* 64-bit bitmap word operations (AND/ANDN/POPC on rows) */
+  uint64_t nodes;             /* search-tree nodes visited (with MCE_FLAG_STATS, else 0) */
+  uint64_t word_ops;          /* bitmap row word operations (AND/ANDN/POPC; with MCE_FLAG_STATS) */
   uint64_t launches;          /* enumeration kernel launches */
   uint64_t warp_cycles[6];    /* warp clock cycles by phase: root build, register tiers,
                                  general tier, exposing tasks, idle, queue */

@@ -30,7 +30,7 @@ PHASES = 6
 OK, ERR_INVALID_ARG, ERR_CAPACITY, ERR_IO, ERR_FORMAT, ERR_NO_DEVICE, ERR_CUDA, ERR_OUT_OF_MEMORY, \
     ERR_TIMEOUT, ERR_TOO_LARGE, ERR_BUSY, ERR_NOT_FOUND, ERR_INTERNAL = range(13)
 ORDER_DEGENERACY, ORDER_UNCHANGED, ORDER_DEGREE_ASC, ORDER_DEGREE_DESC = range(4)
-FLAG_NO_SHARING, FLAG_PER_ROOT, FLAG_QUIET = 1, 2, 4
+FLAG_NO_SHARING, FLAG_PER_ROOT, FLAG_QUIET, FLAG_STATS = 1, 2, 4, 8
 PHASE_H2D, PHASE_PREPROCESS, PHASE_SETUP, PHASE_ENUMERATE, PHASE_D2H, PHASE_TOTAL = range(6)
 
 

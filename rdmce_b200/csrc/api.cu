@@ -328,6 +328,7 @@ static mce_status solve_impl(mce_graph *g, const mce_options &o, mce_result *out
   cfg.reg_share_bound = o.reg_share_bound;
   cfg.expand_r = o.expand_r;
   cfg.sharing = (o.flags & MCE_FLAG_NO_SHARING) ? 0 : 1;
+  cfg.stats = (o.flags & MCE_FLAG_STATS) ? 1 : 0;
   cfg.root_begin = o.root_begin;
   cfg.root_end = o.root_end;
   cfg.spin_limit = spin_of(o);

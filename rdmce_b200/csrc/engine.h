@@ -46,6 +46,7 @@ struct EnumConfig {
   uint32_t reg_share_bound = 0;  // 0 = default
   int expand_r = 1;
   int sharing = 1;
+  int stats = 0;  // count nodes and word-ops (a slower kernel instance)
   uint64_t root_begin = 0, root_end = 0;
   uint64_t spin_limit = 0;
   const uint64_t *root_list = nullptr;  // device: explicit root ids (per-root mode)
@@ -99,6 +100,7 @@ struct EnumParams {
   unsigned long long *per_root_checksum;
   int expand_r;
   int sharing;                           // root-down exposure through the task pool
+  int stats;                             // count search-tree nodes and row word-ops
   uint32_t share_bound;                  // expose only levels with |P| >= this (general tier)
   uint32_t reg_share_bound;              // the same inside the register tiers
   uint32_t nwarps;

@@ -99,12 +99,21 @@ struct WarpSmem {
   uint64_t fP[kT1Depth], fVP[kT1Depth], fs1[kT1Depth], fs2[kT1Depth];
   uint32_t frs[kT1Depth];
   uint8_t fab[kT1Depth][32];
-  // 32-bit tier frames: (P, VP, active rows, |R|) and (s1, s2)
+  // 32-bit tier frames: (P, VP, active rows, R as a column mask)
   uint4 t0f[kT0Depth];
-  ulonglong2 t0s[kT0Depth];
-  // exchange buffer for moving a subproblem into the 32-bit tier
+  // exchange buffer for moving a subproblem into the 32-bit tier; xh1/xh2
+  // hold the label hashes of the running 32-bit-tier subproblem's columns
   uint32_t xrow[32], xcv[32];
   uint64_t xh1[32], xh2[32];
+  // the running 32-bit-tier subproblem's hash sums and |R| at entry, and the
+  // R masks of leaves not yet hashed
+  uint64_t t0_s1, t0_s2;
+  uint32_t t0_rsize;
+  uint32_t pend_rm[32];
+  uint64_t lchk[32];  // per-lane checksum accumulators (batched leaves)
+  // a 32-bit-tier solve that stepped out to expose work: its node state
+  uint32_t y_P, y_VP, y_A, y_RM, y_npend;
+  int y_level;
   uint32_t hcache[kHistCache];
   // result accumulators for the current slot
   unsigned long long count, checksum, nodes, wops;
@@ -145,6 +154,10 @@ __device__ __forceinline__ uint32_t ld_cg(const uint32_t *p) { return __ldcg((co
 __device__ __forceinline__ void acc_flush(const Ctx &c) {
   const EnumParams &P = *c.P;
   WarpSmem *sm = c.sm;
+  __syncwarp();
+  const uint64_t lc = warp_sum_u64(sm->lchk[c.lane]);
+  sm->lchk[c.lane] = 0;
+  if (c.lane == 0) sm->checksum += lc;
   __syncwarp();
   for (uint32_t b = c.lane; b < kHistCache; b += 32) {
     const uint32_t n = sm->hcache[b];
@@ -359,15 +372,18 @@ __device__ __forceinline__ void compress_row(const uint64_t *row, const uint64_t
 // is running; true if anything was exposed.  Defined after those tiers.
 __device__ __noinline__ bool spawn_outer_gen(Ctx c);
 __device__ __noinline__ bool spawn_outer_t1(Ctx c);
-// Exposure from inside the 32-bit tier: enclosing tiers first, then its own
-// levels.  One out-of-line call keeps the node loop's registers free.
+// Exposure for a 32-bit-tier solve that stepped out: enclosing tiers first,
+// then its own levels.
 struct T0;
 __device__ __noinline__ void t0_share(Ctx c, const T0 t, int level);
 
 // ---------------------------------------------------------- 32-bit tier
 // At most 32 candidate columns and 32 rows: lane l holds row l as a 32-bit
-// word (rows 0..pc-1 are the column vertices, the rest X rows) plus the label
-// hashes of column l; P, VP and the active-row set are warp-uniform masks.
+// word (rows 0..pc-1 are the column vertices, the rest X rows).  P, VP, the
+// active-row set and R -- the columns added since the subproblem began -- are
+// warp-uniform masks, so a child costs a few bitwise ops and two ballots.
+// Label-hash sums are not carried down the tree: a leaf records its R mask,
+// and every 32 leaves the lanes hash one clique each (t0_flush).
 
 struct T0 {
   uint32_t row;
@@ -375,14 +391,58 @@ struct T0 {
   uint64_t h1, h2;  // label hashes of column lane
 };
 
+// Hash the pending leaves, one per lane: sums of the entry sums and the R
+// columns' hashes, then the clique hash, histogram and largest size.
+__device__ __forceinline__ void t0_flush(const Ctx &c, uint32_t npend, uint64_t s10, uint64_t s20,
+                                         uint32_t rsize0) {
+  WarpSmem *sm = c.sm;
+  const uint32_t lane = c.lane;
+  __syncwarp();
+  uint32_t size = 0;
+  if (lane < npend) {
+    uint32_t rm = sm->pend_rm[lane];
+    size = rsize0 + 2 + __popc(rm);
+    uint64_t a = s10, b = s20;
+    while (rm) {
+      const uint32_t i = __ffs(rm) - 1;
+      rm &= rm - 1;
+      a += sm->xh1[i];
+      b += sm->xh2[i];
+    }
+    sm->lchk[lane] += clique_hash(a, b, size);
+    if (size < kHistCache) {
+      atomicAdd(&sm->hcache[size], 1u);
+    } else {
+      const EnumParams &P = *c.P;
+      const uint32_t bin = size < P.hist_len ? size : P.hist_len - 1;
+      atomicAdd(&P.hist[(uint64_t)sm->slot * P.hist_len + bin], 1ULL);
+    }
+  }
+  const uint32_t mx = __reduce_max_sync(kFull, size);
+  if (lane == 0) {
+    sm->count += npend;
+    sm->pending += npend;
+    sm->max_size = max(sm->max_size, mx);
+  }
+  __syncwarp();
+}
+
+// hash sums of a frame's R mask (lanes of R contribute their column hash)
+__device__ __forceinline__ void t0_sums(const Ctx &c, uint32_t rm, uint64_t *s1, uint64_t *s2) {
+  const bool in = (rm >> c.lane) & 1;
+  *s1 = c.sm->t0_s1 + warp_sum_u64(in ? c.sm->xh1[c.lane] : 0);
+  *s2 = c.sm->t0_s2 + warp_sum_u64(in ? c.sm->xh2[c.lane] : 0);
+}
+
 // Child task of candidate q at a 32-bit-tier level, as a W = 1 record.
-__device__ void t0_materialize(const Ctx &c, const T0 &t, uint32_t Pbase, uint32_t A, uint32_t q, uint32_t rsize,
-                               uint64_t s1, uint64_t s2, char *rec) {
+__device__ void t0_materialize(const Ctx &c, const T0 &t, uint32_t Pbase, uint32_t A, uint32_t q, uint32_t RM,
+                               char *rec) {
   const uint32_t lane = c.lane;
   const uint32_t CP = Pbase & __shfl_sync(kFull, t.row, q);
   const uint32_t pc = __popc(CP);
   const CPlan plan = compress_plan(CP);
-  const uint64_t hq1 = __shfl_sync(kFull, t.h1, q), hq2 = __shfl_sync(kFull, t.h2, q);
+  uint64_t s1, s2;
+  t0_sums(c, RM | (1u << q), &s1, &s2);
   uint32_t *colv = (uint32_t *)(rec + kHdr);
   uint64_t *rows = (uint64_t *)(rec + kHdr + align8(4ULL * pc));
   const uint64_t cr = compress_apply(t.row, plan);
@@ -399,9 +459,9 @@ __device__ void t0_materialize(const Ctx &c, const T0 &t, uint32_t Pbase, uint32
     h->pc = pc;
     h->nrows = pc + __popc(bal);
     h->W = 1;
-    h->rsize = rsize + 1;
-    h->s1 = s1 + hq1;
-    h->s2 = s2 + hq2;
+    h->rsize = c.sm->t0_rsize + __popc(RM) + 1;
+    h->s1 = s1;
+    h->s2 = s2;
     h->slot = c.sm->slot;
   }
   __syncwarp();
@@ -421,7 +481,6 @@ __device__ void t0_spawn(const Ctx &c, const T0 &t, int level) {
   }
   if (!open) return;
   const uint4 f = sm->t0f[l];
-  const ulonglong2 hs = sm->t0s[l];
   uint32_t VPl = f.y;
   // Highest candidate first: the child of q excludes every open candidate
   // below q, all still open at that point; whatever stays with this warp is
@@ -433,7 +492,7 @@ __device__ void t0_spawn(const Ctx &c, const T0 &t, int level) {
     uint32_t blk;
     if (!pool_alloc(c, &blk)) break;
     const uint32_t Pbase = f.x & ~(VPl & ((1u << q) - 1));
-    t0_materialize(c, t, Pbase, f.z, q, f.w, hs.x, hs.y, pool_block(*c.P, blk));
+    t0_materialize(c, t, Pbase, f.z, q, f.w, pool_block(*c.P, blk));
     pool_publish(c, blk);
     VPl &= ~(1u << q);
   }
@@ -441,31 +500,64 @@ __device__ void t0_spawn(const Ctx &c, const T0 &t, int level) {
   __syncwarp();
 }
 
-__device__ __noinline__ void t0_solve_body(Ctx c, T0 t, uint32_t pc, uint32_t nrows, uint32_t rsize0, uint64_t s10,
-                                           uint64_t s20) {
+// kStats: count search-tree nodes and row word-ops (a separate instance, so
+// the counting costs nothing when it is off)
+//
+// The node loop makes no calls, which keeps its registers free.  To expose
+// work it steps out instead: it saves its state and returns true; the caller
+// (t0_run) exposes levels and calls it again with resume set.
+template <bool kStats>
+__device__ __noinline__ bool t0_solve_body(Ctx c, T0 t, uint32_t pc, uint32_t nrows, uint32_t rsize0, uint64_t s10,
+                                           uint64_t s20, bool resume) {
   const uint32_t lane = c.lane;
   WarpSmem *sm = c.sm;
   const bool expand_r = c.P->expand_r != 0;
-  uint32_t A = nrows >= 32 ? ~0u : ((1u << nrows) - 1);
-  uint32_t P = pc >= 32 ? ~0u : ((1u << pc) - 1);
-  uint32_t VP = 0, rsize = rsize0;
-  uint64_t s1 = s10, s2 = s20;
+  uint32_t A, P, VP, RM, npend;
+  int level;
+  if (!resume) {
+    sm->xh1[lane] = t.h1;
+    sm->xh2[lane] = t.h2;
+    if (lane == 0) {
+      sm->t0_s1 = s10;
+      sm->t0_s2 = s20;
+      sm->t0_rsize = rsize0;
+    }
+    __syncwarp();
+    A = nrows >= 32 ? ~0u : ((1u << nrows) - 1);
+    P = pc >= 32 ? ~0u : ((1u << pc) - 1);
+    VP = 0;
+    RM = 0;
+    npend = 0;
+    level = 0;
+  } else {
+    P = sm->y_P;
+    VP = sm->y_VP;
+    A = sm->y_A;
+    RM = sm->y_RM;
+    npend = sm->y_npend;
+    level = sm->y_level;
+  }
   const uint32_t lanebit = 1u << lane;
   unsigned long long nodes = 0, wops = 0;  // uniform across lanes
-  int level = 0;
   bool fresh = true;
   uint32_t tick = 0;
   for (;;) {
     if (fresh) {
-      nodes++;
+      if (kStats) nodes++;
       if (P == 0) {
-        if (A == 0 && lane == 0) emit(c, rsize + 2, s1, s2);
+        if (A == 0) {  // no row contains R: R is a maximal clique
+          if (lane == 0) sm->pend_rm[npend] = RM;
+          if (++npend == 32) {
+            t0_flush(c, 32, s10, s20, rsize0);
+            npend = 0;
+          }
+        }
         goto backtrack;
       }
       {
         const uint32_t key = (A & lanebit) ? (((uint32_t)__popc(P & ~t.row) << 5) | lane) : 0xffffffffu;
         const uint32_t kmin = __reduce_min_sync(kFull, key);
-        wops += 2 * __popc(A);  // ANDN + POPC per active row
+        if (kStats) wops += 2 * __popc(A);  // ANDN + POPC per active row
         if ((kmin >> 5) == 0) goto backtrack;  // an X row covers P: nothing maximal below
         VP = P & ~__shfl_sync(kFull, t.row, kmin & 31);
         fresh = false;
@@ -476,37 +568,46 @@ __device__ __noinline__ void t0_solve_body(Ctx c, T0 t, uint32_t pc, uint32_t nr
       if (cand == 0) goto backtrack;
       const uint32_t q = __ffs(cand) - 1;
       P &= ~(1u << q);
-      sm->t0f[level] = make_uint4(P, VP, A, rsize);
-      sm->t0s[level] = make_ulonglong2(s1, s2);
+      sm->t0f[level] = make_uint4(P, VP, A, RM);
       uint32_t P2 = P & __shfl_sync(kFull, t.row, q);
-      uint64_t n1 = s1 + __shfl_sync(kFull, t.h1, q);
-      uint64_t n2 = s2 + __shfl_sync(kFull, t.h2, q);
-      uint32_t rs = rsize + 1, M = 1u << q;
+      uint32_t M = 1u << q;
       if (expand_r && __popc(P2) > 1) {
+        // EXPAND_R: a candidate adjacent to all other candidates but itself
+        // joins R at once
         const bool e = (P2 & lanebit) && __popc(P2 & ~t.row) == 1;
         const uint32_t E = __ballot_sync(kFull, e);
-        wops += 2 * __popc(P2);
-        if (E) {
-          P2 &= ~E;
-          M |= E;
-          rs += __popc(E);
-          n1 += warp_sum_u64(e ? t.h1 : 0);
-          n2 += warp_sum_u64(e ? t.h2 : 0);
-        }
+        if (kStats) wops += 2 * __popc(P2);
+        P2 &= ~E;
+        M |= E;
       }
       const uint32_t A2 = A & __ballot_sync(kFull, (t.row & M) == M);
-      wops += __popc(A) + 1;
+      if (kStats) wops += __popc(A) + 1;
       level++;
       P = P2;
       VP = 0;
       A = A2;
-      rsize = rs;
-      s1 = n1;
-      s2 = n2;
+      RM |= M;
       fresh = true;
       if (c.sharing && ++tick >= 128) {
         tick = 0;
-        if (hungry(c)) t0_share(c, t, level);
+        if (hungry(c)) {
+          // step out at this fresh node; t0_run exposes work and resumes
+          __syncwarp();
+          if (lane == 0) {
+            sm->y_P = P;
+            sm->y_VP = VP;
+            sm->y_A = A;
+            sm->y_RM = RM;
+            sm->y_npend = npend;
+            sm->y_level = level;
+            if (kStats) {
+              sm->nodes += nodes;
+              sm->wops += wops;
+            }
+          }
+          __syncwarp();
+          return true;
+        }
       }
       continue;
     }
@@ -515,29 +616,40 @@ __device__ __noinline__ void t0_solve_body(Ctx c, T0 t, uint32_t pc, uint32_t nr
     level--;
     {
       const uint4 f = sm->t0f[level];
-      const ulonglong2 hs = sm->t0s[level];
       P = f.x;
       VP = f.y;
       A = f.z;
-      rsize = f.w;
-      s1 = hs.x;
-      s2 = hs.y;
+      RM = f.w;
     }
     fresh = false;
   }
-  if (lane == 0) {
+  if (npend) t0_flush(c, npend, s10, s20, rsize0);
+  if (kStats && lane == 0) {
     sm->nodes += nodes;
     sm->wops += wops;
   }
   __syncwarp();
   maybe_flush(c);
+  return false;
+}
+
+__device__ __forceinline__ void t0_run(const Ctx &c, const T0 &t, uint32_t pc, uint32_t nrows, uint32_t rsize0,
+                                       uint64_t s10, uint64_t s20) {
+  bool resume = false;
+  for (;;) {
+    const bool out = c.P->stats ? t0_solve_body<true>(c, t, pc, nrows, rsize0, s10, s20, resume)
+                                : t0_solve_body<false>(c, t, pc, nrows, rsize0, s10, s20, resume);
+    if (!out) break;
+    t0_share(c, t, c.sm->y_level);
+    resume = true;
+  }
 }
 
 // timed wrapper: cycles go to the register-tier phase, spawning excluded
 __device__ __forceinline__ void t0_solve(const Ctx &c, const T0 &t, uint32_t pc, uint32_t nrows, uint32_t rsize0,
                                          uint64_t s10, uint64_t s20) {
   const unsigned long long t0 = now(), sp0 = c.sm->cyc[kCycSpawn];
-  t0_solve_body(c, t, pc, nrows, rsize0, s10, s20);
+  t0_run(c, t, pc, nrows, rsize0, s10, s20);
   if (c.lane == 0) c.sm->cyc[kCycReg] += (now() - t0) - (c.sm->cyc[kCycSpawn] - sp0);
 }
 
@@ -791,7 +903,7 @@ __device__ __noinline__ void t1_solve_body(Ctx c, T1 t, uint32_t pc, uint32_t nr
         t0.h2 = lane < pc2 ? sm->xh2[lane] : 0;
         if (lane == 0) sm->t1_level = level;
         __syncwarp();
-        t0_solve_body(c, t0, pc2, nact, rs, n1, n2);
+        t0_run(c, t0, pc2, nact, rs, n1, n2);
         // the child may have exposed open candidates of this level
         VP = sm->fVP[level];
         // While the child ran, the levels above it were exposed only through
@@ -1566,6 +1678,9 @@ __global__ void __launch_bounds__(256, 2) k_enumerate(const __grid_constant__ En
     sm->count = sm->checksum = sm->nodes = sm->wops = 0;
     sm->max_size = sm->slot = sm->pending = 0;
     sm->nest = 0;
+  }
+  sm->lchk[c.lane] = 0;
+  if (c.lane == 0) {
     for (int i = 0; i < kCycPhases; i++) sm->cyc[i] = 0;
   }
   __shared__ unsigned int s_poll;  // the block's poll token (see the idle loop)
@@ -1622,9 +1737,16 @@ __global__ void __launch_bounds__(256, 2) k_enumerate(const __grid_constant__ En
             atomicExch(P.error, 2u);
           }
         }
-        if (P.per_root_count && c.lane == 0) {
-          P.per_root_count[k] = fit ? sm->count - c0 : ~0ULL;
-          P.per_root_checksum[k] = sm->checksum - h0;
+        if (P.per_root_count) {
+          // fold the per-lane checksums of batched leaves into this root's
+          const uint64_t lc = warp_sum_u64(sm->lchk[c.lane]);
+          sm->lchk[c.lane] = 0;
+          __syncwarp();
+          if (c.lane == 0) {
+            sm->checksum += lc;
+            P.per_root_count[k] = fit ? sm->count - c0 : ~0ULL;
+            P.per_root_checksum[k] = sm->checksum - h0;
+          }
         }
         __syncwarp();
         continue;
@@ -1692,8 +1814,10 @@ __global__ void __launch_bounds__(256, 2) k_enumerate(const __grid_constant__ En
   acc_flush(c);
   if (c.lane == 0) {
     atomicAdd(P.stat_roots, nroots);
-    atomicAdd(P.stat_nodes, sm->nodes);
-    atomicAdd(P.stat_wops, sm->wops);
+    if (P.stats) {
+      atomicAdd(P.stat_nodes, sm->nodes);
+      atomicAdd(P.stat_wops, sm->wops);
+    }
     for (int i = 0; i < kCycPhases; i++) atomicAdd(P.stat_cycles + i, sm->cyc[i]);
   }
 }
@@ -1782,6 +1906,7 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
   P.per_root_checksum = cfg.per_root_checksum;
   P.spin_limit = cfg.spin_limit ? cfg.spin_limit : (1ULL << 34);
   P.sharing = (cfg.sharing && cfg.per_root_count == nullptr) ? 1 : 0;
+  P.stats = cfg.stats;
   P.share_bound = cfg.share_bound ? cfg.share_bound : 24;
   P.reg_share_bound = std::min(P.share_bound, cfg.reg_share_bound ? cfg.reg_share_bound : kRegShareBound);
   mce_status s = MCE_OK;
