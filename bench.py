@@ -271,7 +271,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     clocks.start()
     l0 = mce.launch_count()
-    times, enum_ms, wops, nodes, launches_enum = [], 0.0, 0, 0, 0
+    times, enum_ms, launches_enum = [], 0.0, 0
     cycles = [0] * 6
     cliques = 0
     for _ in range(args.steps):
@@ -282,8 +282,6 @@ def run_ours(args):
         times.append(ms)
         cliques += r.count
         enum_ms += r.phase_ms[mce.PHASE_ENUMERATE]
-        wops += r.word_ops
-        nodes += r.nodes
         launches_enum += r.launches
         cycles = [a + b for a, b in zip(cycles, r.warp_cycles)]
     torch.cuda.synchronize()
@@ -332,8 +330,17 @@ def run_ours(args):
     e2e_max = reduce(sum(e2e_times) / 1000.0, _max_op())
     e2e_value = total_cliques / e2e_max
 
+    # The timed kernel counts nothing.  One untimed solve of the same sample
+    # with MCE_FLAG_STATS (a separate kernel instance) counts the search-tree
+    # nodes and row word-ops a step performs: the roofline's algorithmic work.
+    o_stats = mce.options(device=local, stream=C.c_void_p(stream.cuda_stream), flags=mce.FLAG_STATS)
+    rs = g.solve(o_stats) if full and world == 1 else g.solve_root_list(roots, o_stats)
+    if (rs.count, rs.checksum) != ref:
+        raise RuntimeError("counting run differs from the timed runs")
+    wops, nodes = rs.word_ops, rs.nodes
+    enum_ms_step = enum_ms / args.steps
     peak = mce.probe_int_peak(local)
-    achieved = wops / (enum_ms / 1000.0) if enum_ms > 0 else 0.0
+    achieved = wops / (enum_ms_step / 1000.0) if enum_ms_step > 0 else 0.0
 
     line = None
     if rank == 0:
@@ -350,15 +357,16 @@ def run_ours(args):
                        "parallelism": f"{world} rank(s), independent root samples"},
             "roofline": {"bound": "int", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gword-ops/s",
                          "frac": achieved / peak if peak else None, "traffic": None,
-                         "note": "64-bit bitmap row word-ops (ANDN+POPC per active row per node, row filters) of "
-                                 "k_enumerate / its event-timed duration; peak = live INT-pipe probe of the same "
-                                 "op mix on this GPU"},
+                         "note": "bitmap row word-ops of one step (ANDN+POPC per active row per node, row "
+                                 "filters; counted by an untimed MCE_FLAG_STATS solve of the same sample) / the "
+                                 "timed k_enumerate time per step; peak = live INT-pipe probe of the same op mix"},
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": int(u.nbytes + v.nbytes + (0 if full and world == 1 else roots.nbytes)),
                     "d2h_bytes_per_step": int(C.sizeof(mce._Result))},
             "gpu_launches": int(launches),
             "clocks": clk,
-            "search": {"nodes_per_s": nodes / (enum_ms / 1000.0) if enum_ms else None,
+            "search": {"nodes_per_step": int(nodes), "word_ops_per_step": int(wops),
+                       "nodes_per_s": nodes / (enum_ms_step / 1000.0) if enum_ms_step else None,
                        "enumerate_ms_per_step": enum_ms / args.steps,
                        "enum_launches_per_step": launches_enum / args.steps,
                        "warp_cycle_share": {k: round(c / max(1, sum(cycles)), 4) for k, c in
