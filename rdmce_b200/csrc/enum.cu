@@ -1666,7 +1666,7 @@ __device__ void solve_block(const Ctx &c, uint32_t blk) {
   gen_solve(c, G, rsize, s1, s2);
 }
 
-__global__ void __launch_bounds__(256, 2) k_enumerate(const __grid_constant__ EnumParams P) {
+__global__ void __launch_bounds__(256, 3) k_enumerate(const __grid_constant__ EnumParams P) {
   extern __shared__ uint64_t smem_raw[];
   Ctx c;
   c.P = &P;
@@ -1885,7 +1885,7 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
   int sms = 0;
   MCE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
   const uint32_t wpb = cfg.warps_per_block ? std::min(cfg.warps_per_block, 8u) : 8u;
-  const uint32_t bps = cfg.blocks_per_sm ? std::min(cfg.blocks_per_sm, 2u) : 2u;
+  const uint32_t bps = cfg.blocks_per_sm ? std::min(cfg.blocks_per_sm, 3u) : 3u;
   EnumParams &P = plan->params;
   P = EnumParams{};
   P.g.n = g.n;
