@@ -73,7 +73,7 @@ typedef struct mce_options {
   uint64_t spin_limit;        /* bound on every device-side wait; 0 = default */
   void *stream;               /* cudaStream_t to run on; NULL = the engine's own stream */
   uint32_t flags;             /* MCE_FLAG_* */
-  uint32_t reg_share_bound;   /* tau inside the register tiers (<= 64 columns); 0 = 12, never above share_bound */
+  uint32_t reg_share_bound;   /* tau inside the register tiers (<= 64 columns); 0 = 24, never above share_bound */
   uint32_t reserved[6];
 } mce_options;
 

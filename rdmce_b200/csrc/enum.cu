@@ -54,10 +54,11 @@ constexpr uint32_t kT1Depth = 66;         // 64-bit tier: levels (<= 64 columns 
 constexpr uint32_t kT0Depth = 34;         // 32-bit tier: levels (<= 32 columns + root)
 constexpr uint32_t kHdr = 64;             // task record header bytes
 constexpr uint32_t kLocalRec = 2048;      // per-warp local task record (64-bit-tier size)
-// Default tau inside the register tiers.  Their levels have at most 64 (T1)
-// or 32 (T0) candidates, so the general tier's tau of 24 would leave most of
-// their subtrees unshareable.
-constexpr uint32_t kRegShareBound = 12;
+// Default tau inside the register tiers (64 or fewer candidates): the same 24
+// as the general tier measured as fast as smaller values on R-MAT inputs,
+// with fewer, larger tasks, once nested tiers expose their outer levels first.
+constexpr uint32_t kRegShareBound = 24;
+constexpr uint32_t kShareMin = 128, kShareMax = 8192;
 // phases of the per-warp cycle accounting
 enum { kCycBuild = 0, kCycReg = 1, kCycGen = 2, kCycSpawn = 3, kCycIdle = 4, kCycQueue = 5, kCycPhases = 6 };
 
@@ -95,10 +96,6 @@ struct Gen {
 // passed by value.
 struct WarpSmem {
   uint64_t rowbuf[64];
-  // 64-bit tier frames
-  uint64_t fP[kT1Depth], fVP[kT1Depth], fs1[kT1Depth], fs2[kT1Depth];
-  uint32_t frs[kT1Depth];
-  uint8_t fab[kT1Depth][32];
   // 32-bit tier frames: (P, VP, active rows, R as a column mask)
   uint4 t0f[kT0Depth];
   // exchange buffer for moving a subproblem into the 32-bit tier; xh1/xh2
@@ -114,17 +111,19 @@ struct WarpSmem {
   // a 32-bit-tier solve that stepped out to expose work: its node state
   uint32_t y_P, y_VP, y_A, y_RM, y_npend;
   int y_level;
+  // nodes between the 32-bit tier's checks for idle warps; doubles (up to
+  // kShareMax) while checks find nothing to expose, back to kShareMin after
+  // one does
+  uint32_t share_period;
   uint32_t hcache[kHistCache];
   // result accumulators for the current slot
   unsigned long long count, checksum, nodes, wops;
   uint32_t max_size, slot, pending, pad;
   unsigned long long cyc[kCycPhases];  // clock64 cycles by phase
   // The tiers enclosing the running subproblem.  A nested tier exposes their
-  // open levels (shallower, so larger) before its own: rows and column ids of
-  // the running 64-bit-tier solve, the running general-tier solve, and the
-  // level each of them is expanding.
-  uint64_t t1rows[kT1Rows];
-  uint32_t t1cv[64];
+  // open levels (shallower, so larger) before its own: the running
+  // general-tier solve, and the level each enclosing tier is expanding (the
+  // 64-bit tier's rows are in its T1Area).
   Gen gen;
   int t1_level, gen_level;
   uint32_t t1_pc;
@@ -133,9 +132,23 @@ struct WarpSmem {
 
 constexpr uint32_t kNestGen = 1, kNestT1 = 2;
 
+// The 64-bit tier's frames and rows live at the tail of the warp's slab, not
+// in shared memory: that tier holds few of the nodes, and shared memory kept
+// small lets 4 blocks of 8 warps share an SM.
+struct T1Area {
+  uint64_t fP[kT1Depth], fVP[kT1Depth], fs1[kT1Depth], fs2[kT1Depth];
+  uint32_t frs[kT1Depth];
+  uint8_t fab[kT1Depth][32];
+  uint64_t t1rows[kT1Rows];
+  uint32_t t1cv[64];
+};
+constexpr uint32_t kT1Area = (sizeof(T1Area) + 255) & ~255u;
+constexpr uint32_t kTail = kLocalRec + kT1Area;  // slab bytes reserved at its end
+
 struct Ctx {
   const EnumParams *P;
   WarpSmem *sm;
+  T1Area *ta;
   char *slab;
   uint64_t slab_bytes;
   uint32_t lane;
@@ -375,7 +388,7 @@ __device__ __noinline__ bool spawn_outer_t1(Ctx c);
 // Exposure for a 32-bit-tier solve that stepped out: enclosing tiers first,
 // then its own levels.
 struct T0;
-__device__ __noinline__ void t0_share(Ctx c, const T0 t, int level);
+__device__ __noinline__ bool t0_share(Ctx c, const T0 t, int level);
 
 // ---------------------------------------------------------- 32-bit tier
 // At most 32 candidate columns and 32 rows: lane l holds row l as a 32-bit
@@ -469,7 +482,7 @@ __device__ void t0_materialize(const Ctx &c, const T0 &t, uint32_t Pbase, uint32
 
 // expose every open candidate of the shallowest open level with |P| >= tau
 // (the reference's TASK_SHARE_BOUND, BkPivotBitBalance.cuh:271-273)
-__device__ void t0_spawn(const Ctx &c, const T0 &t, int level) {
+__device__ bool t0_spawn(const Ctx &c, const T0 &t, int level) {
   WarpSmem *sm = c.sm;
   int l = 0;
   uint32_t open = 0;
@@ -479,7 +492,7 @@ __device__ void t0_spawn(const Ctx &c, const T0 &t, int level) {
     if (open && (uint32_t)__popc(f.x) + 1 >= c.P->reg_share_bound) break;
     open = 0;
   }
-  if (!open) return;
+  if (!open) return false;
   const uint4 f = sm->t0f[l];
   uint32_t VPl = f.y;
   // Highest candidate first: the child of q excludes every open candidate
@@ -498,6 +511,7 @@ __device__ void t0_spawn(const Ctx &c, const T0 &t, int level) {
   }
   if (c.lane == 0) sm->t0f[l].y = VPl;
   __syncwarp();
+  return true;
 }
 
 // kStats: count search-tree nodes and row word-ops (a separate instance, so
@@ -541,6 +555,7 @@ __device__ __noinline__ bool t0_solve_body(Ctx c, T0 t, uint32_t pc, uint32_t nr
   unsigned long long nodes = 0, wops = 0;  // uniform across lanes
   bool fresh = true;
   uint32_t tick = 0;
+  const uint32_t period = sm->share_period;
   for (;;) {
     if (fresh) {
       if (kStats) nodes++;
@@ -588,7 +603,7 @@ __device__ __noinline__ bool t0_solve_body(Ctx c, T0 t, uint32_t pc, uint32_t nr
       A = A2;
       RM |= M;
       fresh = true;
-      if (c.sharing && ++tick >= 128) {
+      if (c.sharing && ++tick >= period) {
         tick = 0;
         if (hungry(c)) {
           // step out at this fresh node; t0_run exposes work and resumes
@@ -640,7 +655,9 @@ __device__ __forceinline__ void t0_run(const Ctx &c, const T0 &t, uint32_t pc, u
     const bool out = c.P->stats ? t0_solve_body<true>(c, t, pc, nrows, rsize0, s10, s20, resume)
                                 : t0_solve_body<false>(c, t, pc, nrows, rsize0, s10, s20, resume);
     if (!out) break;
-    t0_share(c, t, c.sm->y_level);
+    const bool any = t0_share(c, t, c.sm->y_level);
+    if (c.lane == 0) c.sm->share_period = any ? kShareMin : min(c.sm->share_period * 2, kShareMax);
+    __syncwarp();
     resume = true;
   }
 }
@@ -758,21 +775,33 @@ __device__ void t1_materialize(const Ctx &c, const T1 &t, uint64_t Pbase, uint32
   __syncwarp();
 }
 
+// shallowest 64-bit-tier level below `level` with open candidates and
+// |P| >= tau, or -1
+__device__ __forceinline__ int t1_open_level(const Ctx &c, int level) {
+  const T1Area *ta = c.ta;
+  for (int l = 0; l < level; l++) {
+    const uint64_t Pl = ta->fP[l];
+    if ((Pl & ta->fVP[l]) && (uint32_t)__popcll(Pl) + 1 >= c.P->reg_share_bound) return l;
+  }
+  return -1;
+}
+
 __device__ bool t1_spawn(const Ctx &c, const T1 &t, int level) {
+  T1Area *ta = c.ta;
   WarpSmem *sm = c.sm;
   int l = 0;
   uint64_t open = 0;
   for (; l < level; l++) {
-    open = sm->fP[l] & sm->fVP[l];
-    if (open && (uint32_t)__popcll(sm->fP[l]) + 1 >= c.P->reg_share_bound) break;
+    open = ta->fP[l] & ta->fVP[l];
+    if (open && (uint32_t)__popcll(ta->fP[l]) + 1 >= c.P->reg_share_bound) break;
     open = 0;
   }
   if (!open) return false;
-  const uint64_t Pl = sm->fP[l];
-  uint64_t VPl = sm->fVP[l];
-  const uint32_t abl = sm->fab[l][c.lane];
-  const uint32_t rs = sm->frs[l];
-  const uint64_t s1 = sm->fs1[l], s2 = sm->fs2[l];
+  const uint64_t Pl = ta->fP[l];
+  uint64_t VPl = ta->fVP[l];
+  const uint32_t abl = ta->fab[l][c.lane];
+  const uint32_t rs = ta->frs[l];
+  const uint64_t s1 = ta->fs1[l], s2 = ta->fs2[l];
   // highest open candidate first (see t0_spawn)
   while (open) {
     const uint32_t q = 63 - __clzll((long long)open);
@@ -784,13 +813,14 @@ __device__ bool t1_spawn(const Ctx &c, const T1 &t, int level) {
     pool_publish(c, blk);
     VPl &= ~(1ULL << q);
   }
-  if (c.lane == 0) sm->fVP[l] = VPl;
+  if (c.lane == 0) ta->fVP[l] = VPl;
   __syncwarp();
   return true;
 }
 
 __device__ __noinline__ void t1_solve_body(Ctx c, T1 t, uint32_t pc, uint32_t nrows, uint32_t rsize0, uint64_t s10,
                                            uint64_t s20) {
+  T1Area *ta = c.ta;
   const uint32_t lane = c.lane;
   WarpSmem *sm = c.sm;
   const bool expand_r = c.P->expand_r != 0;
@@ -802,9 +832,9 @@ __device__ __noinline__ void t1_solve_body(Ctx c, T1 t, uint32_t pc, uint32_t nr
   uint64_t VP = 0;
   uint32_t rsize = rsize0;
 #pragma unroll
-  for (int j = 0; j < kRPL; j++) sm->t1rows[32 * j + lane] = t.r[j];
-  sm->t1cv[lane] = t.cva;
-  sm->t1cv[lane + 32] = t.cvb;
+  for (int j = 0; j < kRPL; j++) ta->t1rows[32 * j + lane] = t.r[j];
+  ta->t1cv[lane] = t.cva;
+  ta->t1cv[lane + 32] = t.cvb;
   if (lane == 0) {
     sm->t1_pc = pc;
     sm->nest |= kNestT1;
@@ -840,13 +870,13 @@ __device__ __noinline__ void t1_solve_body(Ctx c, T1 t, uint32_t pc, uint32_t nr
       const uint32_t q = __ffsll((long long)cand) - 1;
       P &= ~(1ULL << q);
       if (lane == 0) {
-        sm->fP[level] = P;
-        sm->fVP[level] = VP;
-        sm->frs[level] = rsize;
-        sm->fs1[level] = s1;
-        sm->fs2[level] = s2;
+        ta->fP[level] = P;
+        ta->fVP[level] = VP;
+        ta->frs[level] = rsize;
+        ta->fs1[level] = s1;
+        ta->fs2[level] = s2;
       }
-      sm->fab[level][lane] = (uint8_t)ab;
+      ta->fab[level][lane] = (uint8_t)ab;
       uint64_t P2 = P & bcast_row(t, q);
       uint64_t n1 = s1 + __shfl_sync(kFull, q < 32 ? t.h1a : t.h1b, q & 31);
       uint64_t n2 = s2 + __shfl_sync(kFull, q < 32 ? t.h2a : t.h2b, q & 31);
@@ -905,7 +935,7 @@ __device__ __noinline__ void t1_solve_body(Ctx c, T1 t, uint32_t pc, uint32_t nr
         __syncwarp();
         t0_run(c, t0, pc2, nact, rs, n1, n2);
         // the child may have exposed open candidates of this level
-        VP = sm->fVP[level];
+        VP = ta->fVP[level];
         // While the child ran, the levels above it were exposed only through
         // the child's own checks; offer them here as well.
         if (c.sharing && ++tick >= 4) {
@@ -914,7 +944,7 @@ __device__ __noinline__ void t1_solve_body(Ctx c, T1 t, uint32_t pc, uint32_t nr
             const unsigned long long ts = now();
             if (!spawn_outer_gen(c)) t1_spawn(c, t, level + 1);
             if (lane == 0) sm->cyc[kCycSpawn] += now() - ts;
-            VP = sm->fVP[level];
+            VP = ta->fVP[level];
           }
         }
         continue;  // next candidate at this level
@@ -940,12 +970,12 @@ __device__ __noinline__ void t1_solve_body(Ctx c, T1 t, uint32_t pc, uint32_t nr
   backtrack:
     if (level == 0) break;
     level--;
-    P = sm->fP[level];
-    VP = sm->fVP[level];
-    rsize = sm->frs[level];
-    s1 = sm->fs1[level];
-    s2 = sm->fs2[level];
-    ab = sm->fab[level][lane];
+    P = ta->fP[level];
+    VP = ta->fVP[level];
+    rsize = ta->frs[level];
+    s1 = ta->fs1[level];
+    s2 = ta->fs2[level];
+    ab = ta->fab[level][lane];
     fresh = false;
   }
   wops = warp_sum_u64(wops);
@@ -1126,7 +1156,7 @@ __device__ __noinline__ void gen_solve_body(Ctx c, Gen G, uint32_t rsize0, uint6
   uint64_t *stack = G.stack;
   uint32_t *alist = G.alist;
   const uint64_t *rows = G.rows;
-  char *local = c.slab + c.slab_bytes - kLocalRec;
+  char *local = c.slab + c.slab_bytes - kLocalRec;  // inside kTail, after the T1Area
   unsigned long long nodes = 0, wops = 0;
   if (lane == 0) {
     sm->gen = G;
@@ -1399,20 +1429,23 @@ __device__ __noinline__ bool spawn_outer_gen(Ctx c) {
 
 __device__ __noinline__ bool spawn_outer_t1(Ctx c) {
   WarpSmem *sm = c.sm;
+  T1Area *ta = c.ta;
   if (!(sm->nest & kNestT1)) return false;
+  if (t1_open_level(c, sm->t1_level + 1) < 0) return false;  // before loading rows
   T1 t;
 #pragma unroll
-  for (int j = 0; j < kRPL; j++) t.r[j] = sm->t1rows[32 * j + c.lane];
-  t.cva = sm->t1cv[c.lane];
-  t.cvb = sm->t1cv[c.lane + 32];
+  for (int j = 0; j < kRPL; j++) t.r[j] = ta->t1rows[32 * j + c.lane];
+  t.cva = ta->t1cv[c.lane];
+  t.cvb = ta->t1cv[c.lane + 32];
   t1_hashes(c, t, sm->t1_pc);
   return t1_spawn(c, t, sm->t1_level + 1);
 }
 
-__device__ __noinline__ void t0_share(Ctx c, const T0 t, int level) {
+__device__ __noinline__ bool t0_share(Ctx c, const T0 t, int level) {
   const unsigned long long ts = now();
-  if (!spawn_outer_gen(c) && !spawn_outer_t1(c)) t0_spawn(c, t, level);
+  const bool any = spawn_outer_gen(c) || spawn_outer_t1(c) || t0_spawn(c, t, level);
   if (c.lane == 0) c.sm->cyc[kCycSpawn] += now() - ts;
+  return any;
 }
 
 __device__ __forceinline__ void gen_solve(const Ctx &c, const Gen &G, uint32_t rsize0, uint64_t s10, uint64_t s20) {
@@ -1524,7 +1557,7 @@ __host__ __device__ __forceinline__ Layout layout_for(uint64_t cand_n, uint32_t 
   L.stack_off = L.rows_off + 8ULL * (uint64_t)nrows * W;
   // pc + 1 levels, one scratch record past the deepest, one spare
   L.alist_off = L.stack_off + 8ULL * (uint64_t)(pc + 3) * (3ULL * W + 4);
-  L.need = L.alist_off + 4ULL * nrows + kLocalRec;
+  L.need = L.alist_off + 4ULL * nrows + kTail;
   return L;
 }
 
@@ -1534,7 +1567,7 @@ __device__ bool solve_root(const Ctx &c, uint64_t r) {
   const uint32_t v0 = g.root_v0[r], v1 = g.root_v1[r];
   set_slot(c, g.slot ? g.slot[v0] : 0);
   uint32_t *cand = (uint32_t *)c.slab;
-  const uint64_t cap = (c.slab_bytes - kLocalRec) / 4;
+  const uint64_t cap = (c.slab_bytes - kTail) / 4;
   const unsigned long long tb0 = now();
   const uint32_t nc = intersect(g, v0, v1, cand, cap);
   if (nc == 0xffffffffu) {
@@ -1597,7 +1630,7 @@ __device__ bool solve_root(const Ctx &c, uint64_t r) {
   G.h2s = h2s;
   G.stack = (uint64_t *)(c.slab + L.stack_off);
   G.alist = (uint32_t *)(c.slab + L.alist_off);
-  G.alist_cap = (c.slab_bytes - kLocalRec - L.alist_off) / 4;
+  G.alist_cap = (c.slab_bytes - kTail - L.alist_off) / 4;
   G.pc = p;
   G.nrows = nrows;
   G.W = W;
@@ -1658,7 +1691,7 @@ __device__ void solve_block(const Ctx &c, uint32_t blk) {
   G.h2s = h2s;
   G.stack = (uint64_t *)(c.slab + L.stack_off);
   G.alist = (uint32_t *)(c.slab + L.alist_off);
-  G.alist_cap = (c.slab_bytes - kLocalRec - L.alist_off) / 4;
+  G.alist_cap = (c.slab_bytes - kTail - L.alist_off) / 4;
   G.pc = pc;
   G.nrows = nrows;
   G.W = W;
@@ -1666,7 +1699,7 @@ __device__ void solve_block(const Ctx &c, uint32_t blk) {
   gen_solve(c, G, rsize, s1, s2);
 }
 
-__global__ void __launch_bounds__(256, 3) k_enumerate(const __grid_constant__ EnumParams P) {
+__global__ void __launch_bounds__(256, 4) k_enumerate(const __grid_constant__ EnumParams P) {
   extern __shared__ uint64_t smem_raw[];
   Ctx c;
   c.P = &P;
@@ -1678,6 +1711,7 @@ __global__ void __launch_bounds__(256, 3) k_enumerate(const __grid_constant__ En
     sm->count = sm->checksum = sm->nodes = sm->wops = 0;
     sm->max_size = sm->slot = sm->pending = 0;
     sm->nest = 0;
+    sm->share_period = kShareMin;
   }
   sm->lchk[c.lane] = 0;
   if (c.lane == 0) {
@@ -1689,6 +1723,7 @@ __global__ void __launch_bounds__(256, 3) k_enumerate(const __grid_constant__ En
   const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   c.slab = P.slab + gwarp * P.slab_bytes;
   c.slab_bytes = P.slab_bytes;
+  c.ta = (T1Area *)(c.slab + c.slab_bytes - kTail);
   c.sharing = P.sharing != 0;
   const bool range_mode = P.heavy_list == nullptr && P.root_list == nullptr;
   const uint64_t total = range_mode ? P.re - P.rb : P.n_list;
@@ -1885,7 +1920,7 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
   int sms = 0;
   MCE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
   const uint32_t wpb = cfg.warps_per_block ? std::min(cfg.warps_per_block, 8u) : 8u;
-  const uint32_t bps = cfg.blocks_per_sm ? std::min(cfg.blocks_per_sm, 3u) : 3u;
+  const uint32_t bps = cfg.blocks_per_sm ? std::min(cfg.blocks_per_sm, 4u) : 4u;
   EnumParams &P = plan->params;
   P = EnumParams{};
   P.g.n = g.n;
@@ -1952,6 +1987,7 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
   const uint64_t bound = align8(LB.need + 3ULL * (kcap + dcap) * 4);
   uint64_t slab_bytes = std::max<uint64_t>(std::min<uint64_t>(bound, 4ULL << 20), 16ULL << 10);
   while (slab_bytes > (64ULL << 10) && slab_bytes * nwarps > freeb / 2) slab_bytes >>= 1;
+  slab_bytes = (slab_bytes + 255) & ~255ULL;  // every warp's slab (and its T1Area) 256-byte aligned
   plan->fits_all = slab_bytes >= bound;
   char *slab = (char *)scr->get(2, slab_bytes * nwarps, &s);
   if (!slab) return s;
@@ -2023,7 +2059,7 @@ mce_status enum_finish(const EnumPlan &plan, cudaStream_t st, EnumStats *stats) 
     // deferred roots: large slabs, and every warp of the pass shares their work
     size_t freeb = 0, totalb = 0;
     MCE_CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
-    const uint64_t need = align8(h.heavy_need) + 4096;
+    const uint64_t need = ((h.heavy_need + 4096) + 255) & ~255ULL;
     const uint64_t hw = std::min<uint64_t>((uint64_t)(freeb * 0.7) / need, plan.nwarps);
     if (hw == 0) return MCE_ERR_OUT_OF_MEMORY;
     mce_status s = MCE_OK;
