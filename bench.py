@@ -39,7 +39,7 @@ sys.path.insert(0, ROOT)
 SCALE, EDGE_FACTOR, GRAPH_SEED = 20, 16, 2
 SAMPLE_SEED = 12345
 # smaller graphs enumerated in full (profiling and context lines): name -> (scale, edge factor, seed)
-FULL_WORKLOADS = {"rmat14": (14, 16, 1), "rmat16": (16, 16, 1)}
+FULL_WORKLOADS = {"rmat14": (14, 16, 1), "rmat16": (16, 16, 1), "chunglu": None}
 DEFAULT_SAMPLE = int(os.environ.get("RDMCE_BENCH_SAMPLE", "256"))
 METRIC = "maximal cliques/s"
 UNIT = "cliques/s"
@@ -47,6 +47,8 @@ REF_CPU = os.path.join(ROOT, "oracle", "_ref", "ref_cpu")
 
 
 def workload_name(sample, workload="rmat20-sample"):
+    if workload == "chunglu":
+        return "Chung-Lu n=10,000, expected average degree 16, exponent 2.5, seed 1; full enumeration"
     if workload in FULL_WORKLOADS:
         sc, ef, sd = FULL_WORKLOADS[workload]
         return f"R-MAT scale {sc}, edge factor {ef}, a/b/c/d=0.57/0.19/0.19/0.05, seed {sd}; full enumeration"
@@ -114,6 +116,8 @@ def dist_env():
 def make_graph_pairs(workload="rmat20-sample"):
     import rdmce_b200 as mce
 
+    if workload == "chunglu":
+        return mce.gen_chung_lu(10000, 16, 2.5, 1)
     if workload in FULL_WORKLOADS:
         sc, ef, sd = FULL_WORKLOADS[workload]
         return mce.gen_rmat(sc, ef, sd)
