@@ -31,6 +31,7 @@ struct Request {
   std::vector<uint32_t> u, v;
   uint64_t est_bytes = 0;
   int state = 0;  // 0 queued, 1 running, 2 done
+  uint32_t share = 1;  // requests running on the device when this one was admitted (itself included)
   mce_status status = MCE_OK;
   std::unique_ptr<mce_result> result;
   Clock::time_point t_submit, t_done;
@@ -53,6 +54,8 @@ struct mce_server {
 
 namespace mce {
 namespace {
+
+constexpr uint32_t kServeBlocksPerSm = 4;  // the enumeration kernel's residency
 
 uint64_t estimate_bytes(const Request &r) {
   uint32_t maxlab = 0;
@@ -87,8 +90,11 @@ void run_request(mce_server *s, Request *r, cudaStream_t st, Scratch *scr) {
     if (dres && cudaMemsetAsync(dres, 0, res_bytes, st) != cudaSuccess) rc = MCE_ERR_CUDA;
     if (rc == MCE_OK) {
       EnumConfig cfg;
-      const uint32_t inflight = std::max<uint32_t>(1, s->opt.max_inflight);
-      cfg.max_blocks = std::max<uint32_t>(s->sms * 2 / std::min<uint32_t>(inflight, 4), 8);
+      // A request admitted onto an idle device gets the whole GPU; one admitted
+      // beside k others gets 1/(k+1) of it (at least one block per SM), so
+      // concurrent persistent grids fit on the SMs side by side.
+      const uint32_t full = (uint32_t)s->sms * kServeBlocksPerSm;
+      cfg.max_blocks = std::max<uint32_t>(full / std::max<uint32_t>(r->share, 1), (uint32_t)s->sms);
       EnumStats stats;
       rc = enumerate(g, cfg, scr, st, (SlotResult *)dres, (unsigned long long *)(dres + sizeof(SlotResult)), &stats);
       if (rc == MCE_OK) {
@@ -156,6 +162,7 @@ void worker_main(mce_server *s) {
       r->state = 1;
       s->in_use += r->est_bytes;
       s->running++;
+      r->share = s->running;
     }
     run_request(s, r, st, &scr);
     {
@@ -163,8 +170,8 @@ void worker_main(mce_server *s) {
       s->in_use -= r->est_bytes;
       s->running--;
     }
-    // scratch of a finished request goes back to the device for the others
-    scr.release();
+    // The worker keeps its scratch for the next request: freeing device memory
+    // would synchronise the whole device and stall the other requests.
     s->cv_work.notify_all();
     s->cv_done.notify_all();
   }
