@@ -131,6 +131,30 @@ def root_sample(m, sample, rank):
     return np.sort(rng.choice(m, size=min(sample, m), replace=False)).astype(np.uint64)
 
 
+def rank_roots(m, rank, world, full, sample):
+    """The roots one rank enumerates: a contiguous share of all m roots for a
+    full enumeration (the shares partition [0, m)), else the rank's own seeded
+    sample.  Ranks never exchange roots or results on the data path."""
+    import numpy as np
+
+    if full:
+        return np.arange(m * rank // world, m * (rank + 1) // world, dtype=np.uint64)
+    return root_sample(m, sample, rank)
+
+
+def reduce_over_ranks(x, op, world, device):
+    """One all-reduce of a scalar (max of times, sum of counts) for the JSON
+    line; the identity on one rank."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=op)
+    return float(t.item())
+
+
 def emit(line):
     print(json.dumps(line), flush=True)
 
@@ -233,13 +257,7 @@ def run_ours(args):
             dist.barrier()
 
     def reduce(x, op):
-        if world == 1:
-            return x
-        import torch.distributed as dist
-
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=op)
-        return float(t.item())
+        return reduce_over_ranks(x, op, world, dev)
 
     stream = torch.cuda.current_stream(dev)
     o = mce.options(device=local, stream=C.c_void_p(stream.cuda_stream))
@@ -247,12 +265,7 @@ def run_ours(args):
     u, v = make_graph_pairs(args.workload)
     g = mce.Graph.from_coo(u, v, o)
     info = g.info()
-    if full:
-        # every root; ranks split the edge list into contiguous ranges
-        roots = np.arange(info["num_edges"] * rank // world, info["num_edges"] * (rank + 1) // world,
-                          dtype=np.uint64)
-    else:
-        roots = root_sample(info["num_edges"], args.sample, rank)
+    roots = rank_roots(info["num_edges"], rank, world, full, args.sample)
 
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)  # 4x L2
 
