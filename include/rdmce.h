@@ -99,6 +99,8 @@ typedef struct mce_result {
   uint64_t launches;          /* enumeration kernel launches */
   uint64_t warp_cycles[6];    /* warp clock cycles by phase: root build, register tiers,
                                  general tier, exposing tasks, idle, queue */
+  uint64_t max_item_cycles[2]; /* longest single work item, in warp clock cycles: [0] a root,
+                                  [1] a task taken from another warp */
   double phase_ms[MCE_PHASES];
   uint64_t hist[MCE_HIST_LEN];
 } mce_result;

@@ -75,6 +75,7 @@ class _Result(C.Structure):
         ("word_ops", C.c_uint64),
         ("launches", C.c_uint64),
         ("warp_cycles", C.c_uint64 * 6),
+        ("max_item_cycles", C.c_uint64 * 2),
         ("phase_ms", C.c_double * PHASES),
         ("hist", C.c_uint64 * HIST_LEN),
     ]
@@ -128,13 +129,14 @@ class Result:
     launches: int = 0
     # warp clock cycles: root build, register tiers, general tier, exposing tasks, idle, queue
     warp_cycles: list = field(default_factory=list)
+    max_item_cycles: list = field(default_factory=list)
 
     @classmethod
     def _from(cls, r: _Result) -> "Result":
         hist = {s: int(r.hist[s]) for s in range(HIST_LEN) if r.hist[s]}
         return cls(r.count, r.checksum, hist, r.max_size, r.degeneracy, r.max_degree, r.num_vertices,
                    r.num_edges, r.roots, r.shared_tasks, r.heavy_roots, list(r.phase_ms), r.nodes, r.word_ops,
-                   r.launches, list(r.warp_cycles))
+                   r.launches, list(r.warp_cycles), list(r.max_item_cycles))
 
 
 _lib = None

@@ -464,7 +464,8 @@ __device__ void t0_materialize(const Ctx &c, const T0 &t, uint32_t Pbase, uint32
     colv[k] = t.cv;
     rows[k] = cr;
   }
-  const bool isx = ((A >> lane) & 1) && ((t.row >> q) & 1) && !((CP >> lane) & 1);
+  const bool isx = ((A >> lane) & 1) && ((t.row >> q) & 1) && !((CP >> lane) & 1) &&
+                   (CP == 0 || (t.row & CP) != 0);  // X rows empty on the child's columns left out
   const uint32_t bal = __ballot_sync(kFull, isx);
   if (isx) rows[pc + __popc(bal & lanemask_lt())] = cr;
   if (lane == 0) {
@@ -757,7 +758,7 @@ __device__ void t1_materialize(const Ctx &c, const T1 &t, uint64_t Pbase, uint32
     const uint32_t idx = 32 * j + lane;
     const bool act = ((ab >> j) & 1) && ((t.r[j] >> q) & 1);
     const bool isc = idx < 64 && ((CP >> idx) & 1);
-    const bool isx = act && !isc;
+    const bool isx = act && !isc && (CP == 0 || (t.r[j] & CP) != 0);  // empty X rows left out
     const uint32_t bal = __ballot_sync(kFull, isx);
     if (isx) rows[base + __popc(bal & lanemask_lt())] = compress_apply(t.r[j], plan);
     base += __popc(bal);
@@ -903,7 +904,19 @@ __device__ __noinline__ void t1_solve_body(Ctx c, T1 t, uint32_t pc, uint32_t nr
       // A child with <= 32 columns and <= 32 active rows drops to the 32-bit
       // tier: rows compressed to the child's columns and gathered, columns
       // first, through the warp's exchange buffer.
-      const uint32_t nact = __reduce_add_sync(kFull, __popc(ab2));
+      // X rows with no bit on the child's candidates never matter below a
+      // child that has candidates (a pivot among them leaves VP = P, and they
+      // drop out at the next step), so the handoff leaves them out
+      uint32_t ab3 = ab2;
+      if (P2) {
+#pragma unroll
+        for (int j = 0; j < kRPL; j++) {
+          const uint32_t idx = 32 * j + lane;
+          const bool isc = idx < 64 && ((P2 >> idx) & 1);
+          if (!isc && (t.r[j] & P2) == 0) ab3 &= ~(1u << j);
+        }
+      }
+      const uint32_t nact = __reduce_add_sync(kFull, __popc(ab3));
       if (__popcll(P2) <= 32 && nact <= 32) {
         const uint32_t pc2 = __popcll(P2);
         const CPlan plan = compress_plan(P2);
@@ -911,7 +924,7 @@ __device__ __noinline__ void t1_solve_body(Ctx c, T1 t, uint32_t pc, uint32_t nr
 #pragma unroll
         for (int j = 0; j < kRPL; j++) {
           const uint32_t idx = 32 * j + lane;
-          const bool act = (ab2 >> j) & 1;
+          const bool act = (ab3 >> j) & 1;
           const bool isc = idx < 64 && ((P2 >> idx) & 1);
           if (act && isc) {
             const uint32_t k = __popcll(P2 & ((1ULL << idx) - 1));
@@ -1049,13 +1062,21 @@ __device__ bool gen_materialize(const Ctx &c, const Gen &G, const uint64_t *rec_
     return true;
   };
   auto is_col = [&](uint32_t i) -> bool { return i < G.pc && ((CP[i >> 6] >> (i & 63)) & 1); };
+  // X rows empty on the child's columns are left out when it has columns
+  auto hits = [&](uint32_t i) -> bool {
+    if (pc == 0) return true;
+    const uint64_t *row = G.rows + (uint64_t)i * W;
+    for (uint32_t w = 0; w < W; w++)
+      if (row[w] & CP[w]) return true;
+    return false;
+  };
   uint32_t nx = 0;
   for (uint32_t base = 0; base < alen; base += 32) {
     const uint32_t t = base + lane;
     bool x = false;
     if (t < alen) {
       const uint32_t i = aoff == kIdent ? t : G.alist[aoff + t];
-      x = !is_col(i) && keep_row(i);
+      x = !is_col(i) && keep_row(i) && hits(i);
     }
     nx += __popc(__ballot_sync(kFull, x));
   }
@@ -1080,7 +1101,7 @@ __device__ bool gen_materialize(const Ctx &c, const Gen &G, const uint64_t *rec_
     uint32_t i = 0;
     if (t < alen) {
       i = aoff == kIdent ? t : G.alist[aoff + t];
-      x = !is_col(i) && keep_row(i);
+      x = !is_col(i) && keep_row(i) && hits(i);
     }
     const uint32_t bal = __ballot_sync(kFull, x);
     if (x) compress_row(G.rows + (uint64_t)i * W, CP, W, rows + (uint64_t)(pos + __popc(bal & lanemask_lt())) * Wn);
@@ -1298,6 +1319,12 @@ __device__ __noinline__ void gen_solve_body(Ctx c, Gen G, uint32_t rsize0, uint6
           keep = (row[wq] & bq) != 0;
           if (lazy)
             for (uint32_t w = 0; w < W && keep; w++) keep = (R[w] & row[w]) == R[w];
+          // an X row empty on the child's columns is left out of the record
+          if (keep && !(i < G.pc && ((CP[i >> 6] >> (i & 63)) & 1))) {
+            bool hit = false;
+            for (uint32_t w = 0; w < W && !hit; w++) hit = (row[w] & CP[w]) != 0;
+            keep = hit;
+          }
         }
         ccount += __popc(__ballot_sync(kFull, keep));
       }
@@ -1365,6 +1392,7 @@ __device__ __noinline__ void gen_solve_body(Ctx c, Gen G, uint32_t rsize0, uint6
     if ((uint64_t)atop + alen <= G.alist_cap) {
       uint32_t n2 = 0;
       const bool single = !lazy && nE == 0;
+      const bool child_has_p = cpc > nE;  // X rows empty on P' matter only at a leaf
       for (uint32_t base = 0; base < alen; base += 32) {
         const uint32_t t = base + lane;
         bool keep = false;
@@ -1377,6 +1405,11 @@ __device__ __noinline__ void gen_solve_body(Ctx c, Gen G, uint32_t rsize0, uint6
           if (!single) {
             const uint64_t *need = lazy ? CR : CE;
             for (uint32_t w = 0; w < W && keep; w++) keep = (row[w] & need[w]) == need[w];
+          }
+          if (keep && child_has_p && !(i < G.pc && ((CP[i >> 6] >> (i & 63)) & 1))) {
+            bool hit = false;
+            for (uint32_t w = 0; w < W && !hit; w++) hit = (row[w] & CP[w]) != 0;
+            keep = hit;
           }
         }
         const uint32_t bal = __ballot_sync(kFull, keep);
@@ -1747,7 +1780,9 @@ __global__ void __launch_bounds__(256, 4) k_enumerate(const __grid_constant__ En
         const uint32_t blk = __shfl_sync(kFull, b, 0);
         if (c.lane == 0) sm->cyc[kCycQueue] += now() - tq;
         if (got) {
+          const unsigned long long tb = now();
           solve_block(c, blk);
+          if (c.lane == 0) atomicMax(P.stat_max_item + 1, now() - tb);
           continue;
         }
       }
@@ -1761,7 +1796,9 @@ __global__ void __launch_bounds__(256, 4) k_enumerate(const __grid_constant__ En
         else r = P.re - 1 - k;  // late-peeled roots first
         const unsigned long long c0 = sm->count, h0 = sm->checksum;
         nroots++;
+        const unsigned long long tr = now();
         const bool fit = solve_root(c, r);
+        if (c.lane == 0) atomicMax(P.stat_max_item, now() - tr);
         if (!fit && c.lane == 0) {
           if (P.push_heavy) {
             P.heavy_out[atomicAdd(P.heavy_n, 1u)] = (uint32_t)r;
@@ -1838,7 +1875,9 @@ __global__ void __launch_bounds__(256, 4) k_enumerate(const __grid_constant__ En
     }
     got = __shfl_sync(kFull, got, 0);
     if (got) {
+      const unsigned long long tb = now();
       solve_block(c, __shfl_sync(kFull, b, 0));
+      if (c.lane == 0) atomicMax(P.stat_max_item + 1, now() - tb);
       if (c.lane == 0) atomicSub(P.active, 1u);
       idle_spins = 0;
       quiet = 0;
@@ -1867,6 +1906,7 @@ struct EnumCtl {
   alignas(128) unsigned int active;
   alignas(128) unsigned long long heavy_need, stat_roots, stat_tasks, stat_nodes, stat_wops;
   unsigned long long stat_cycles[kCycPhases];
+  unsigned long long stat_max_item[2];
   unsigned int heavy_n, error;
 };
 
@@ -1957,6 +1997,7 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
   P.stat_nodes = &ctl->stat_nodes;
   P.stat_wops = &ctl->stat_wops;
   P.stat_cycles = ctl->stat_cycles;
+  P.stat_max_item = ctl->stat_max_item;
   P.active = &ctl->active;
   P.free_head = &ctl->free_head;
   P.free_tail = &ctl->free_tail;
@@ -2054,6 +2095,7 @@ mce_status enum_finish(const EnumPlan &plan, cudaStream_t st, EnumStats *stats) 
   uint64_t tasks = h.stat_tasks, nodes = h.stat_nodes, wops = h.stat_wops;
   uint64_t cycles[kCycPhases];
   for (int i = 0; i < kCycPhases; i++) cycles[i] = h.stat_cycles[i];
+  uint64_t max_item[2] = {h.stat_max_item[0], h.stat_max_item[1]};
   uint32_t err = h.error;
   if (h.heavy_n && !h.error) {
     // deferred roots: large slabs, and every warp of the pass shares their work
@@ -2089,6 +2131,7 @@ mce_status enum_finish(const EnumPlan &plan, cudaStream_t st, EnumStats *stats) 
     nodes += h2.stat_nodes;
     wops += h2.stat_wops;
     for (int i = 0; i < kCycPhases; i++) cycles[i] += h2.stat_cycles[i];
+    for (int i = 0; i < 2; i++) max_item[i] = std::max<uint64_t>(max_item[i], h2.stat_max_item[i]);
     err = h2.error;
   }
   if (stats) {
@@ -2098,6 +2141,7 @@ mce_status enum_finish(const EnumPlan &plan, cudaStream_t st, EnumStats *stats) 
     stats->nodes = nodes;
     stats->word_ops = wops;
     for (int i = 0; i < kCycPhases; i++) stats->cycles[i] = cycles[i];
+    for (int i = 0; i < 2; i++) stats->max_item[i] = max_item[i];
     stats->error = err;
     stats->launches = launches;
   }
