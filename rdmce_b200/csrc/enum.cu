@@ -527,7 +527,7 @@ __device__ __noinline__ bool t0_solve_body(Ctx c, T0 t, uint32_t pc, uint32_t nr
   const uint32_t lane = c.lane;
   WarpSmem *sm = c.sm;
   const bool expand_r = c.P->expand_r != 0;
-  uint32_t A, P, VP, RM, npend;
+  uint32_t A, P, RM, npend;
   int level;
   if (!resume) {
     sm->xh1[lane] = t.h1;
@@ -540,13 +540,11 @@ __device__ __noinline__ bool t0_solve_body(Ctx c, T0 t, uint32_t pc, uint32_t nr
     __syncwarp();
     A = nrows >= 32 ? ~0u : ((1u << nrows) - 1);
     P = pc >= 32 ? ~0u : ((1u << pc) - 1);
-    VP = 0;
     RM = 0;
     npend = 0;
     level = 0;
   } else {
     P = sm->y_P;
-    VP = sm->y_VP;
     A = sm->y_A;
     RM = sm->y_RM;
     npend = sm->y_npend;
@@ -554,90 +552,93 @@ __device__ __noinline__ bool t0_solve_body(Ctx c, T0 t, uint32_t pc, uint32_t nr
   }
   const uint32_t lanebit = 1u << lane;
   unsigned long long nodes = 0, wops = 0;  // uniform across lanes
-  bool fresh = true;
   uint32_t tick = 0;
   const uint32_t period = sm->share_period;
-  for (;;) {
-    if (fresh) {
+  // A child whose candidate set comes out empty is a leaf: it is tested where
+  // it is made, without a frame push, a descent and a backtrack.
+  uint32_t VP = 0;
+node:  // a node with candidates P, active rows A and R = RM
+  if (kStats) nodes++;
+  if (P == 0) {  // only a subproblem without columns starts like this
+    if (A == 0) {
+      if (lane == 0) sm->pend_rm[npend] = RM;
+      ++npend;
+    }
+    goto backtrack;
+  }
+  {
+    const uint32_t key = (A & lanebit) ? (((uint32_t)__popc(P & ~t.row) << 5) | lane) : 0xffffffffu;
+    const uint32_t kmin = __reduce_min_sync(kFull, key);
+    if (kStats) wops += 2 * __popc(A);  // ANDN + POPC per active row
+    if ((kmin >> 5) == 0) goto backtrack;  // an X row covers P: nothing maximal below
+    VP = P & ~__shfl_sync(kFull, t.row, kmin & 31);
+  }
+expand:  // next candidate of VP at this level
+  {
+    const uint32_t cand = P & VP;
+    if (cand == 0) goto backtrack;
+    const uint32_t q = __ffs(cand) - 1;
+    P &= ~(1u << q);
+    uint32_t P2 = P & __shfl_sync(kFull, t.row, q);
+    uint32_t M = 1u << q;
+    if (expand_r && (P2 & (P2 - 1))) {
+      // EXPAND_R: a candidate adjacent to every other candidate joins R at
+      // once; rows carry no self bit, so that is P2 \ row == {itself}
+      const uint32_t E = __ballot_sync(kFull, (P2 & ~t.row) == lanebit);
+      if (kStats) wops += 2 * __popc(P2);
+      P2 &= ~E;
+      M |= E;
+    }
+    const uint32_t A2 = A & __ballot_sync(kFull, (t.row & M) == M);
+    if (kStats) wops += __popc(A) + 1;
+    if (P2 == 0) {  // leaf child: maximal iff no row contains R + M
       if (kStats) nodes++;
-      if (P == 0) {
-        if (A == 0) {  // no row contains R: R is a maximal clique
-          if (lane == 0) sm->pend_rm[npend] = RM;
-          if (++npend == 32) {
-            t0_flush(c, 32, s10, s20, rsize0);
-            npend = 0;
-          }
-        }
-        goto backtrack;
-      }
-      {
-        const uint32_t key = (A & lanebit) ? (((uint32_t)__popc(P & ~t.row) << 5) | lane) : 0xffffffffu;
-        const uint32_t kmin = __reduce_min_sync(kFull, key);
-        if (kStats) wops += 2 * __popc(A);  // ANDN + POPC per active row
-        if ((kmin >> 5) == 0) goto backtrack;  // an X row covers P: nothing maximal below
-        VP = P & ~__shfl_sync(kFull, t.row, kmin & 31);
-        fresh = false;
-      }
-    }
-    {
-      const uint32_t cand = P & VP;
-      if (cand == 0) goto backtrack;
-      const uint32_t q = __ffs(cand) - 1;
-      P &= ~(1u << q);
-      sm->t0f[level] = make_uint4(P, VP, A, RM);
-      uint32_t P2 = P & __shfl_sync(kFull, t.row, q);
-      uint32_t M = 1u << q;
-      if (expand_r && __popc(P2) > 1) {
-        // EXPAND_R: a candidate adjacent to all other candidates but itself
-        // joins R at once
-        const bool e = (P2 & lanebit) && __popc(P2 & ~t.row) == 1;
-        const uint32_t E = __ballot_sync(kFull, e);
-        if (kStats) wops += 2 * __popc(P2);
-        P2 &= ~E;
-        M |= E;
-      }
-      const uint32_t A2 = A & __ballot_sync(kFull, (t.row & M) == M);
-      if (kStats) wops += __popc(A) + 1;
-      level++;
-      P = P2;
-      VP = 0;
-      A = A2;
-      RM |= M;
-      fresh = true;
-      if (c.sharing && ++tick >= period) {
-        tick = 0;
-        if (hungry(c)) {
-          // step out at this fresh node; t0_run exposes work and resumes
-          __syncwarp();
-          if (lane == 0) {
-            sm->y_P = P;
-            sm->y_VP = VP;
-            sm->y_A = A;
-            sm->y_RM = RM;
-            sm->y_npend = npend;
-            sm->y_level = level;
-            if (kStats) {
-              sm->nodes += nodes;
-              sm->wops += wops;
-            }
-          }
-          __syncwarp();
-          return true;
+      if (A2 == 0) {
+        if (lane == 0) sm->pend_rm[npend] = RM | M;
+        if (++npend == 32) {
+          t0_flush(c, 32, s10, s20, rsize0);
+          npend = 0;
         }
       }
-      continue;
+      goto expand;
     }
-  backtrack:
-    if (level == 0) break;
+    sm->t0f[level] = make_uint4(P, VP, A, RM);
+    level++;
+    P = P2;
+    A = A2;
+    RM |= M;
+    if (c.sharing && ++tick >= period) {
+      tick = 0;
+      if (hungry(c)) {
+        // step out at this fresh node; t0_run exposes work and resumes
+        __syncwarp();
+        if (lane == 0) {
+          sm->y_P = P;
+          sm->y_VP = 0;
+          sm->y_A = A;
+          sm->y_RM = RM;
+          sm->y_npend = npend;
+          sm->y_level = level;
+          if (kStats) {
+            sm->nodes += nodes;
+            sm->wops += wops;
+          }
+        }
+        __syncwarp();
+        return true;
+      }
+    }
+    goto node;
+  }
+backtrack:
+  if (level > 0) {
     level--;
-    {
-      const uint4 f = sm->t0f[level];
-      P = f.x;
-      VP = f.y;
-      A = f.z;
-      RM = f.w;
-    }
-    fresh = false;
+    const uint4 f = sm->t0f[level];
+    P = f.x;
+    VP = f.y;
+    A = f.z;
+    RM = f.w;
+    goto expand;
   }
   if (npend) t0_flush(c, npend, s10, s20, rsize0);
   if (kStats && lane == 0) {
