@@ -566,6 +566,19 @@ node:  // a node with candidates P, active rows A and R = RM
     }
     goto backtrack;
   }
+  if ((P & (P - 1)) == 0) {
+    // One candidate q: R + q is maximal iff no active row holds q (the pivot
+    // step would prune on such a row, else branch on q into a leaf).
+    if (kStats) nodes++;
+    if ((A & __ballot_sync(kFull, (t.row & P) != 0)) == 0) {
+      if (lane == 0) sm->pend_rm[npend] = RM | P;
+      if (++npend == 32) {
+        t0_flush(c, 32, s10, s20, rsize0);
+        npend = 0;
+      }
+    }
+    goto backtrack;
+  }
   {
     const uint32_t key = (A & lanebit) ? (((uint32_t)__popc(P & ~t.row) << 5) | lane) : 0xffffffffu;
     const uint32_t kmin = __reduce_min_sync(kFull, key);
