@@ -580,6 +580,35 @@ node:  // a node with candidates P, active rows A and R = RM
     goto backtrack;
   }
   {
+    const uint32_t lo = P & (0u - P), hi = P & ~lo;
+    if (hi == (hi & (0u - hi))) {
+      // Two candidates a, b.  Adjacent: R + a + b is the only maximal clique
+      // below, iff no active row holds both.  Not adjacent: R + a and R + b
+      // each are, iff no active row holds that vertex.  (What the pivot and
+      // the two branches would find.)
+      if (kStats) nodes++;
+      const uint32_t ra = A & __ballot_sync(kFull, (t.row & lo) != 0);
+      const uint32_t rb = A & __ballot_sync(kFull, (t.row & hi) != 0);
+      const uint32_t a = __ffs(lo) - 1;
+      uint32_t emit_rm[2];
+      uint32_t ne = 0;
+      if (__shfl_sync(kFull, t.row, a) & hi) {
+        if ((ra & rb) == 0) emit_rm[ne++] = RM | P;
+      } else {
+        if (ra == 0) emit_rm[ne++] = RM | lo;
+        if (rb == 0) emit_rm[ne++] = RM | hi;
+      }
+      for (uint32_t k = 0; k < ne; k++) {
+        if (lane == 0) sm->pend_rm[npend] = emit_rm[k];
+        if (++npend == 32) {
+          t0_flush(c, 32, s10, s20, rsize0);
+          npend = 0;
+        }
+      }
+      goto backtrack;
+    }
+  }
+  {
     const uint32_t key = (A & lanebit) ? (((uint32_t)__popc(P & ~t.row) << 5) | lane) : 0xffffffffu;
     const uint32_t kmin = __reduce_min_sync(kFull, key);
     if (kStats) wops += 2 * __popc(A);  // ANDN + POPC per active row
