@@ -59,6 +59,7 @@ constexpr uint32_t kLocalRec = 2048;      // per-warp local task record (64-bit-
 // with fewer, larger tasks, once nested tiers expose their outer levels first.
 constexpr uint32_t kRegShareBound = 24;
 constexpr uint32_t kShareMin = 128, kShareMax = 8192;
+constexpr int kSmallP = 5;  // 32-bit-tier nodes with this few candidates are decided in one step
 // phases of the per-warp cycle accounting
 enum { kCycBuild = 0, kCycReg = 1, kCycGen = 2, kCycSpawn = 3, kCycIdle = 4, kCycQueue = 5, kCycPhases = 6 };
 
@@ -607,6 +608,43 @@ node:  // a node with candidates P, active rows A and R = RM
       }
       goto backtrack;
     }
+  }
+  if (__popc(P) <= kSmallP) {
+    // Few candidates: R + K is a maximal clique for exactly the cliques K of
+    // the candidates that no active row contains (a candidate outside K that
+    // extends K is itself such a row).  Lane i tests the i-th subset of P.
+    if (kStats) nodes++;
+    const uint32_t n = __popc(P);
+    uint32_t pm = P, qbit[kSmallP], adj[kSmallP], holds[kSmallP];
+#pragma unroll
+    for (int k = 0; k < kSmallP; k++) {
+      qbit[k] = pm & (0u - pm);
+      pm &= pm - 1;
+      adj[k] = qbit[k] ? (__shfl_sync(kFull, t.row, __ffs(qbit[k] | 0x80000000u) - 1) & P) : 0;
+      holds[k] = A & __ballot_sync(kFull, (t.row & qbit[k]) != 0);
+    }
+    uint32_t mask = 0, rows = ~0u;
+    bool clique = true;
+#pragma unroll
+    for (int k = 0; k < kSmallP; k++)
+      if ((lane >> k) & 1) {
+        mask |= qbit[k];
+        rows &= holds[k];
+      }
+#pragma unroll
+    for (int k = 0; k < kSmallP; k++)
+      if ((lane >> k) & 1) clique = clique && ((adj[k] & mask) == (mask & ~qbit[k]));
+    const bool out = lane != 0 && lane < (1u << n) && clique && rows == 0;
+    const uint32_t E = __ballot_sync(kFull, out);
+    const uint32_t pos = npend + __popc(E & lanemask_lt());
+    if (out && pos < 32) sm->pend_rm[pos] = RM | mask;
+    npend += __popc(E);
+    if (npend >= 32) {
+      t0_flush(c, 32, s10, s20, rsize0);
+      if (out && pos >= 32) sm->pend_rm[pos - 32] = RM | mask;
+      npend -= 32;
+    }
+    goto backtrack;
   }
   {
     const uint32_t key = (A & lanebit) ? (((uint32_t)__popc(P & ~t.row) << 5) | lane) : 0xffffffffu;
