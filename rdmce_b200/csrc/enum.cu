@@ -516,6 +516,90 @@ __device__ bool t0_spawn(const Ctx &c, const T0 &t, int level) {
   return true;
 }
 
+// A node with 1 to kSmallP candidates P, active rows A and R = RM, decided
+// in one step: its maximal cliques go to the pending leaves.
+__device__ __forceinline__ void t0_small(const Ctx &c, const T0 &t, uint32_t P, uint32_t A, uint32_t RM,
+                                         uint32_t &npend, uint64_t s10, uint64_t s20, uint32_t rsize0) {
+  WarpSmem *sm = c.sm;
+  const uint32_t lane = c.lane;
+  if ((P & (P - 1)) == 0) {
+    // One candidate q: R + q is maximal iff no active row holds q (the pivot
+    // step would prune on such a row, else branch on q into a leaf).
+    if ((A & __ballot_sync(kFull, (t.row & P) != 0)) == 0) {
+      if (lane == 0) sm->pend_rm[npend] = RM | P;
+      if (++npend == 32) {
+        t0_flush(c, 32, s10, s20, rsize0);
+        npend = 0;
+      }
+    }
+    return;
+  }
+  {
+    const uint32_t lo = P & (0u - P), hi = P & ~lo;
+    if (hi == (hi & (0u - hi))) {
+      // Two candidates a, b.  Adjacent: R + a + b is the only maximal clique
+      // below, iff no active row holds both.  Not adjacent: R + a and R + b
+      // each are, iff no active row holds that vertex.  (What the pivot and
+      // the two branches would find.)
+      const uint32_t ra = A & __ballot_sync(kFull, (t.row & lo) != 0);
+      const uint32_t rb = A & __ballot_sync(kFull, (t.row & hi) != 0);
+      const uint32_t a = __ffs(lo) - 1;
+      uint32_t emit_rm[2];
+      uint32_t ne = 0;
+      if (__shfl_sync(kFull, t.row, a) & hi) {
+        if ((ra & rb) == 0) emit_rm[ne++] = RM | P;
+      } else {
+        if (ra == 0) emit_rm[ne++] = RM | lo;
+        if (rb == 0) emit_rm[ne++] = RM | hi;
+      }
+      for (uint32_t k = 0; k < ne; k++) {
+        if (lane == 0) sm->pend_rm[npend] = emit_rm[k];
+        if (++npend == 32) {
+          t0_flush(c, 32, s10, s20, rsize0);
+          npend = 0;
+        }
+      }
+      return;
+    }
+  }
+  {
+    // Few candidates: R + K is a maximal clique for exactly the cliques K of
+    // the candidates that no active row contains (a candidate outside K that
+    // extends K is itself such a row).  Lane i tests the i-th subset of P.
+    const uint32_t n = __popc(P);
+    uint32_t pm = P, qbit[kSmallP], adj[kSmallP], holds[kSmallP];
+#pragma unroll
+    for (int k = 0; k < kSmallP; k++) {
+      qbit[k] = pm & (0u - pm);
+      pm &= pm - 1;
+      adj[k] = qbit[k] ? (__shfl_sync(kFull, t.row, __ffs(qbit[k] | 0x80000000u) - 1) & P) : 0;
+      holds[k] = A & __ballot_sync(kFull, (t.row & qbit[k]) != 0);
+    }
+    uint32_t mask = 0, rows = ~0u;
+    bool clique = true;
+#pragma unroll
+    for (int k = 0; k < kSmallP; k++)
+      if ((lane >> k) & 1) {
+        mask |= qbit[k];
+        rows &= holds[k];
+      }
+#pragma unroll
+    for (int k = 0; k < kSmallP; k++)
+      if ((lane >> k) & 1) clique = clique && ((adj[k] & mask) == (mask & ~qbit[k]));
+    const bool out = lane != 0 && lane < (1u << n) && clique && rows == 0;
+    const uint32_t E = __ballot_sync(kFull, out);
+    const uint32_t pos = npend + __popc(E & lanemask_lt());
+    if (out && pos < 32) sm->pend_rm[pos] = RM | mask;
+    npend += __popc(E);
+    if (npend >= 32) {
+      t0_flush(c, 32, s10, s20, rsize0);
+      if (out && pos >= 32) sm->pend_rm[pos - 32] = RM | mask;
+      npend -= 32;
+    }
+    return;
+  }
+}
+
 // kStats: count search-tree nodes and row word-ops (a separate instance, so
 // the counting costs nothing when it is off)
 //
@@ -567,83 +651,9 @@ node:  // a node with candidates P, active rows A and R = RM
     }
     goto backtrack;
   }
-  if ((P & (P - 1)) == 0) {
-    // One candidate q: R + q is maximal iff no active row holds q (the pivot
-    // step would prune on such a row, else branch on q into a leaf).
-    if (kStats) nodes++;
-    if ((A & __ballot_sync(kFull, (t.row & P) != 0)) == 0) {
-      if (lane == 0) sm->pend_rm[npend] = RM | P;
-      if (++npend == 32) {
-        t0_flush(c, 32, s10, s20, rsize0);
-        npend = 0;
-      }
-    }
-    goto backtrack;
-  }
-  {
-    const uint32_t lo = P & (0u - P), hi = P & ~lo;
-    if (hi == (hi & (0u - hi))) {
-      // Two candidates a, b.  Adjacent: R + a + b is the only maximal clique
-      // below, iff no active row holds both.  Not adjacent: R + a and R + b
-      // each are, iff no active row holds that vertex.  (What the pivot and
-      // the two branches would find.)
-      if (kStats) nodes++;
-      const uint32_t ra = A & __ballot_sync(kFull, (t.row & lo) != 0);
-      const uint32_t rb = A & __ballot_sync(kFull, (t.row & hi) != 0);
-      const uint32_t a = __ffs(lo) - 1;
-      uint32_t emit_rm[2];
-      uint32_t ne = 0;
-      if (__shfl_sync(kFull, t.row, a) & hi) {
-        if ((ra & rb) == 0) emit_rm[ne++] = RM | P;
-      } else {
-        if (ra == 0) emit_rm[ne++] = RM | lo;
-        if (rb == 0) emit_rm[ne++] = RM | hi;
-      }
-      for (uint32_t k = 0; k < ne; k++) {
-        if (lane == 0) sm->pend_rm[npend] = emit_rm[k];
-        if (++npend == 32) {
-          t0_flush(c, 32, s10, s20, rsize0);
-          npend = 0;
-        }
-      }
-      goto backtrack;
-    }
-  }
   if (__popc(P) <= kSmallP) {
-    // Few candidates: R + K is a maximal clique for exactly the cliques K of
-    // the candidates that no active row contains (a candidate outside K that
-    // extends K is itself such a row).  Lane i tests the i-th subset of P.
     if (kStats) nodes++;
-    const uint32_t n = __popc(P);
-    uint32_t pm = P, qbit[kSmallP], adj[kSmallP], holds[kSmallP];
-#pragma unroll
-    for (int k = 0; k < kSmallP; k++) {
-      qbit[k] = pm & (0u - pm);
-      pm &= pm - 1;
-      adj[k] = qbit[k] ? (__shfl_sync(kFull, t.row, __ffs(qbit[k] | 0x80000000u) - 1) & P) : 0;
-      holds[k] = A & __ballot_sync(kFull, (t.row & qbit[k]) != 0);
-    }
-    uint32_t mask = 0, rows = ~0u;
-    bool clique = true;
-#pragma unroll
-    for (int k = 0; k < kSmallP; k++)
-      if ((lane >> k) & 1) {
-        mask |= qbit[k];
-        rows &= holds[k];
-      }
-#pragma unroll
-    for (int k = 0; k < kSmallP; k++)
-      if ((lane >> k) & 1) clique = clique && ((adj[k] & mask) == (mask & ~qbit[k]));
-    const bool out = lane != 0 && lane < (1u << n) && clique && rows == 0;
-    const uint32_t E = __ballot_sync(kFull, out);
-    const uint32_t pos = npend + __popc(E & lanemask_lt());
-    if (out && pos < 32) sm->pend_rm[pos] = RM | mask;
-    npend += __popc(E);
-    if (npend >= 32) {
-      t0_flush(c, 32, s10, s20, rsize0);
-      if (out && pos >= 32) sm->pend_rm[pos - 32] = RM | mask;
-      npend -= 32;
-    }
+    t0_small(c, t, P, A, RM, npend, s10, s20, rsize0);
     goto backtrack;
   }
   {
@@ -680,6 +690,11 @@ expand:  // next candidate of VP at this level
           npend = 0;
         }
       }
+      goto expand;
+    }
+    if (__popc(P2) <= kSmallP) {  // small child: decided here, no descent
+      if (kStats) nodes++;
+      t0_small(c, t, P2, A2, RM | M, npend, s10, s20, rsize0);
       goto expand;
     }
     sm->t0f[level] = make_uint4(P, VP, A, RM);
