@@ -18,15 +18,22 @@
 //     most 32 candidate columns and 32 rows that contain R: there each lane
 //     holds one row as a 32-bit word, P / VP / the active-row set are
 //     warp-uniform 32-bit masks, and a node is one redux.sync (pivot argmin),
-//     one ballot (the child's active rows) and a few shuffles.  Up to 64
+//     two ballots (EXPAND_R, the child's active rows) and a few shuffles.  Up to 64
 //     columns and 128 rows, each lane holds 4 rows as 64-bit words.  Larger
 //     subproblems run in the general tier (W 64-bit words per row in a global
 //     scratch slab, per-level lists of active rows).  A child small enough for
 //     a smaller tier has its rows compressed to its own columns (parallel bit
 //     compress) and gathered, and continues there.
+//   * In the 32-bit tier R is a column mask and leaves are hashed 32 at a
+//     time, one per lane.  A node or child with at most 5 candidates is
+//     decided in one step: its maximal cliques are the cliques K of the
+//     candidates that no active row contains, and lane i tests the i-th
+//     subset.  The node loop makes no calls; to expose work it steps out
+//     and is resumed.
 //   * Root-down exposure with self-contained tasks.  When warps are idle, a
-//     busy warp turns every open candidate of its shallowest level with
-//     |P| >= tau into a task record (rows restricted to the child's columns)
+//     busy warp turns every open candidate of the shallowest open level with
+//     |P| >= tau -- outer tiers of a nested solve first -- into a task record
+//     (rows restricted to the child's columns, X rows empty on them left out)
 //     in a global pool, published through lock-free bounded MPMC rings.  A
 //     task owns its data, so no warp ever waits on another warp's stack (the
 //     reference's owner waits for its thieves, :87-138).  Every wait is bounded.
@@ -110,7 +117,7 @@ struct WarpSmem {
   uint32_t pend_rm[32];
   uint64_t lchk[32];  // per-lane checksum accumulators (batched leaves)
   // a 32-bit-tier solve that stepped out to expose work: its node state
-  uint32_t y_P, y_VP, y_A, y_RM, y_npend;
+  uint32_t y_P, y_A, y_RM, y_npend;
   int y_level;
   // nodes between the 32-bit tier's checks for idle warps; doubles (up to
   // kShareMax) while checks find nothing to expose, back to kShareMin after
@@ -709,7 +716,6 @@ expand:  // next candidate of VP at this level
         __syncwarp();
         if (lane == 0) {
           sm->y_P = P;
-          sm->y_VP = 0;
           sm->y_A = A;
           sm->y_RM = RM;
           sm->y_npend = npend;
