@@ -12,7 +12,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "hostio.h"
@@ -53,6 +55,42 @@ bool extract_u32(const char *s, size_t len, size_t &pos, uint32_t &out) {
 
 }  // namespace
 
+namespace {
+
+// One record attempt from a line start: `>> u >> v` (either may cross line
+// breaks), then the rest of the current line is skipped.  Returns the next
+// record start, which is again a line start (or len).
+inline size_t parse_record(const char *s, size_t len, size_t pos, std::vector<uint32_t> &u,
+                           std::vector<uint32_t> &v) {
+  uint32_t a = 0, b = 0;
+  const bool ok = extract_u32(s, len, pos, a) && extract_u32(s, len, pos, b);
+  if (ok) {
+    u.push_back(a);
+    v.push_back(b);
+  }
+  const void *nl = std::memchr(s + pos, '\n', len - pos);
+  return nl ? (size_t)((const char *)nl - s) + 1 : len;
+}
+
+// Parse [from, ...) until the first record start at or past `stop`; returns it.
+size_t parse_span(const char *s, size_t len, size_t from, size_t stop, std::vector<uint32_t> &u,
+                  std::vector<uint32_t> &v) {
+  size_t pos = from;
+  while (pos < stop && pos < len) pos = parse_record(s, len, pos, u, v);
+  return pos;
+}
+
+constexpr size_t kChunkBytes = 4u << 20;  // below this a file is parsed by one thread
+
+}  // namespace
+
+// Record starts form a chain: each is a line start fixed by the one before,
+// and a record normally ends at its own line end.  The file is cut at line
+// starts into chunks parsed in parallel, each assuming a record starts at its
+// first byte.  Then, in order, a chunk whose true first record start (where
+// the previous chunk's chain left off) differs from its cut -- a record ran
+// across the cut -- is parsed again from the true start.  The output is
+// exactly the sequential parse.
 mce_status parse_coo_text(const char *path, std::vector<uint32_t> &u, std::vector<uint32_t> &v) {
   FILE *f = std::fopen(path, "rb");
   if (!f) return MCE_ERR_IO;
@@ -77,18 +115,46 @@ mce_status parse_coo_text(const char *path, std::vector<uint32_t> &u, std::vecto
   const size_t L = (size_t)len;
   u.clear();
   v.clear();
-  u.reserve(L / 8);
-  v.reserve(L / 8);
-  size_t pos = 0;
-  while (pos < L) {
-    uint32_t a = 0, b = 0;
-    bool ok = extract_u32(s, L, pos, a) && extract_u32(s, L, pos, b);
-    if (ok) {
-      u.push_back(a);
-      v.push_back(b);
-    }
-    const void *nl = std::memchr(s + pos, '\n', L - pos);
-    pos = nl ? (size_t)((const char *)nl - s) + 1 : L;
+  size_t nt = std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), L / kChunkBytes));
+  if (nt == 1) {
+    u.reserve(L / 8);
+    v.reserve(L / 8);
+    parse_span(s, L, 0, L, u, v);
+    return MCE_OK;
+  }
+  // cuts at line starts
+  std::vector<size_t> cut(nt + 1);
+  cut[0] = 0;
+  cut[nt] = L;
+  for (size_t j = 1; j < nt; j++) {
+    size_t c = std::max(cut[j - 1], L * j / nt);
+    const void *nl = std::memchr(s + c, '\n', L - c);
+    cut[j] = nl ? (size_t)((const char *)nl - s) + 1 : L;
+  }
+  std::vector<std::vector<uint32_t>> cu(nt), cv(nt);
+  std::vector<size_t> end(nt);
+  std::vector<std::thread> th;
+  for (size_t j = 0; j < nt; j++)
+    th.emplace_back([&, j]() {
+      cu[j].reserve((cut[j + 1] - cut[j]) / 8);
+      cv[j].reserve((cut[j + 1] - cut[j]) / 8);
+      end[j] = parse_span(s, L, cut[j], cut[j + 1], cu[j], cv[j]);
+    });
+  for (auto &t : th) t.join();
+  for (size_t j = 1; j < nt; j++) {
+    if (end[j - 1] == cut[j]) continue;
+    // a record ran across the cut: this chunk restarts where the chain is
+    cu[j].clear();
+    cv[j].clear();
+    end[j] = end[j - 1] >= cut[j + 1] ? end[j - 1] : parse_span(s, L, end[j - 1], cut[j + 1], cu[j], cv[j]);
+  }
+  size_t total = 0;
+  for (size_t j = 0; j < nt; j++) total += cu[j].size();
+  u.reserve(total);
+  v.reserve(total);
+  for (size_t j = 0; j < nt; j++) {
+    u.insert(u.end(), cu[j].begin(), cu[j].end());
+    v.insert(v.end(), cv[j].begin(), cv[j].end());
   }
   return MCE_OK;
 }

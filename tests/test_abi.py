@@ -138,3 +138,36 @@ def test_cli_usage_errors(engine):
     assert r.returncode == 1 and "Usage" in r.stderr
     r = subprocess.run([engine.CLI_PATH, "-i", "x.txt", "-o", "bogus"], capture_output=True, text=True)
     assert r.returncode == 1 and "Usage" in r.stderr
+
+
+@pytest.mark.parametrize("kind", ["one_per_line", "mixed"])
+def test_parallel_parse_matches_sequential_oracle(engine, oracle_mod, tmp_path, kind):
+    """Files of several MB are parsed in parallel chunks; records that run
+    across a chunk cut (a lone number takes its partner from the next line)
+    must come out exactly as a sequential parse gives them."""
+    rng = np.random.default_rng(7)
+    path = str(tmp_path / "big.txt")
+    with open(path, "w") as f:
+        if kind == "one_per_line":
+            f.write("\n".join(str(x) for x in rng.integers(0, 1 << 20, size=2_500_001)))
+        else:
+            lines = []
+            for _ in range(900_000):
+                r = rng.random()
+                a, b = rng.integers(0, 1 << 20, size=2)
+                if r < 0.7:
+                    lines.append(f"{a} {b}")
+                elif r < 0.8:
+                    lines.append(f"{a}")
+                elif r < 0.85:
+                    lines.append("% comment")
+                elif r < 0.9:
+                    lines.append("")
+                else:
+                    lines.append(f"{a}\t{b} extra tokens 5 6")
+            f.write("\n".join(lines))
+    assert os.path.getsize(path) > 8 << 20
+    a = engine.parse_text(path)
+    b = oracle_mod.parse_text(path)
+    assert len(a[0]) > 100_000
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
