@@ -13,6 +13,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <memory>
+#include <new>
 #include <string>
 #include <thread>
 #include <vector>
@@ -94,7 +96,6 @@ constexpr size_t kChunkBytes = 4u << 20;  // below this a file is parsed by one 
 mce_status parse_coo_text(const char *path, std::vector<uint32_t> &u, std::vector<uint32_t> &v) {
   FILE *f = std::fopen(path, "rb");
   if (!f) return MCE_ERR_IO;
-  std::vector<char> buf;
   if (std::fseek(f, 0, SEEK_END) != 0) {
     std::fclose(f);
     return MCE_ERR_IO;
@@ -105,13 +106,17 @@ mce_status parse_coo_text(const char *path, std::vector<uint32_t> &u, std::vecto
     std::fclose(f);
     return MCE_ERR_IO;
   }
-  buf.resize((size_t)len + 1);
-  if (len > 0 && std::fread(buf.data(), 1, (size_t)len, f) != (size_t)len) {
+  std::unique_ptr<char[]> buf(new (std::nothrow) char[(size_t)len + 1]);  // not zero-filled
+  if (!buf) {
+    std::fclose(f);
+    return MCE_ERR_OUT_OF_MEMORY;
+  }
+  if (len > 0 && std::fread(buf.get(), 1, (size_t)len, f) != (size_t)len) {
     std::fclose(f);
     return MCE_ERR_IO;
   }
   std::fclose(f);
-  const char *s = buf.data();
+  const char *s = buf.get();
   const size_t L = (size_t)len;
   u.clear();
   v.clear();
@@ -136,9 +141,14 @@ mce_status parse_coo_text(const char *path, std::vector<uint32_t> &u, std::vecto
   std::vector<std::thread> th;
   for (size_t j = 0; j < nt; j++)
     th.emplace_back([&, j]() {
-      cu[j].reserve((cut[j + 1] - cut[j]) / 8);
-      cv[j].reserve((cut[j + 1] - cut[j]) / 8);
-      end[j] = parse_span(s, L, cut[j], cut[j + 1], cu[j], cv[j]);
+      // thread-local vectors: neighbouring vector headers share cache lines
+      std::vector<uint32_t> lu, lv;
+      lu.reserve((cut[j + 1] - cut[j]) / 8);
+      lv.reserve((cut[j + 1] - cut[j]) / 8);
+      const size_t e = parse_span(s, L, cut[j], cut[j + 1], lu, lv);
+      cu[j] = std::move(lu);
+      cv[j] = std::move(lv);
+      end[j] = e;
     });
   for (auto &t : th) t.join();
   for (size_t j = 1; j < nt; j++) {
@@ -148,14 +158,19 @@ mce_status parse_coo_text(const char *path, std::vector<uint32_t> &u, std::vecto
     cv[j].clear();
     end[j] = end[j - 1] >= cut[j + 1] ? end[j - 1] : parse_span(s, L, end[j - 1], cut[j + 1], cu[j], cv[j]);
   }
-  size_t total = 0;
-  for (size_t j = 0; j < nt; j++) total += cu[j].size();
-  u.reserve(total);
-  v.reserve(total);
-  for (size_t j = 0; j < nt; j++) {
-    u.insert(u.end(), cu[j].begin(), cu[j].end());
-    v.insert(v.end(), cv[j].begin(), cv[j].end());
-  }
+  std::vector<size_t> at(nt + 1, 0);
+  for (size_t j = 0; j < nt; j++) at[j + 1] = at[j] + cu[j].size();
+  u.resize(at[nt]);
+  v.resize(at[nt]);
+  th.clear();
+  for (size_t j = 0; j < nt; j++)
+    th.emplace_back([&, j]() {
+      if (!cu[j].empty()) {
+        std::memcpy(u.data() + at[j], cu[j].data(), cu[j].size() * 4);
+        std::memcpy(v.data() + at[j], cv[j].data(), cv[j].size() * 4);
+      }
+    });
+  for (auto &t : th) t.join();
   return MCE_OK;
 }
 
