@@ -171,3 +171,28 @@ def test_parallel_parse_matches_sequential_oracle(engine, oracle_mod, tmp_path, 
     b = oracle_mod.parse_text(path)
     assert len(a[0]) > 100_000
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_bin_reader_rejects_damaged_files(engine, oracle_mod, tmp_path):
+    """The .bin reader (the reference container) checks its input before any
+    device work: truncated, inconsistent or oversized headers are FORMAT /
+    TOO_LARGE errors, a missing file an IO error."""
+    u, v = engine.gen_rmat(8, 8, 3)
+    g = oracle_mod.Graph.from_pairs(u, v).sort_degeneracy()
+    good = tmp_path / "g.bin"
+    g.store_bin(str(good))
+    raw = good.read_bytes()
+    L = engine.lib()
+    h = C.c_void_p()
+
+    def load(data, name):
+        path = tmp_path / name
+        path.write_bytes(data)
+        return L.mce_graph_load_file(str(path).encode(), None, C.byref(h))
+
+    assert load(raw[:20], "short.bin") == engine.ERR_FORMAT           # header cut
+    assert load(raw[: len(raw) // 2], "half.bin") == engine.ERR_FORMAT  # adjacency cut
+    big = bytearray(raw)
+    big[8:16] = (1 << 31).to_bytes(8, "little")  # m with 2m >= 2^32
+    assert load(bytes(big), "big.bin") == engine.ERR_TOO_LARGE
+    assert L.mce_graph_load_file(str(tmp_path / "missing.bin").encode(), None, C.byref(h)) == engine.ERR_IO
