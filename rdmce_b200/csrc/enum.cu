@@ -891,7 +891,6 @@ __device__ __forceinline__ int t1_open_level(const Ctx &c, int level) {
 
 __device__ bool t1_spawn(const Ctx &c, const T1 &t, int level) {
   T1Area *ta = c.ta;
-  WarpSmem *sm = c.sm;
   int l = 0;
   uint64_t open = 0;
   for (; l < level; l++) {
