@@ -17,8 +17,19 @@ Lines printed (rank 0): one JSON line per the benchmark contract: device-timed
 roofline of the enumeration kernel against a live probe of the INT pipe, and
 the CPU oracle on the host cores as `cpu_baseline`.
 
+Parity.  tests/golden/samples/rmat20_sample.json holds the CPU oracle's answer
+for the headline sample (count, checksum, histogram, per-root values and a
+digest of the ordered CSR); the run fails unless the engine reproduces it.
+
 `--impl reference` times the reference's own CPU solver (oracle/_ref/ref_cpu,
-compiled from the unmodified reference sources) on the host cores.
+compiled from the unmodified reference sources) on the SAME edge roots of the
+same ordered graph: MceSolver::BKFixedMemPivotBit2 with R = {v0, v1}, P and X
+split at v1, as the reference's edge-root loop does (src/mce.cc:96-131).  The
+graph is written as a reference .bin in the engine's vertex order by a
+separate process (oracle/ordered_bin.py), so the timed process loads only the
+reference build.  Before timing, the sample's light roots are solved to
+completion and checked root by root against the fixture; each timed step then
+runs all threads over the sample, heaviest roots first, until its deadline.
 """
 from __future__ import annotations
 
@@ -43,6 +54,24 @@ DEFAULT_SAMPLE = int(os.environ.get("RDMCE_BENCH_SAMPLE", "256"))
 METRIC = "maximal cliques/s"
 UNIT = "cliques/s"
 REF_CPU = os.path.join(ROOT, "oracle", "_ref", "ref_cpu")
+FIXTURE = os.path.join(ROOT, "tests", "golden", "samples", "rmat20_sample.json")
+# roots below this many cliques finish in well under a second on one core:
+# the reference arm solves them to completion as its parity check
+LIGHT_ROOT = 10_000_000
+
+
+def load_fixture():
+    with open(FIXTURE) as f:
+        return json.load(f)
+
+
+def sample_config(fx, sample):
+    """The workload-defining config keys, identical for both arms."""
+    return {"workload": workload_name(sample), "roots_per_step": len(fx["roots"]), "sample_seed": fx["sample_seed"],
+            "vertices": fx["n"], "edges": fx["m"], "degeneracy": fx["degeneracy"], "max_degree": fx["max_degree"],
+            "cliques_per_step": fx["count"], "checksum": fx["checksum"],
+            "l2": "512 MiB device write before every GPU step (L2 is 126 MB)",
+            "parallelism": "1 rank(s), independent root samples"}
 
 
 def workload_name(sample, workload="rmat20-sample"):
@@ -171,52 +200,79 @@ def run_reference(args):
         base["unavailable"] = "oracle/_ref/ref_cpu (the reference CPU solver) was not built on this machine"
         emit(base)
         return 0
-    import numpy as np
-
-    u, v = make_graph_pairs()
+    fx = load_fixture()
+    if args.sample != len(fx["roots"]):
+        base["unavailable"] = f"the reference arm runs the fixture's {len(fx['roots'])}-root sample only"
+        emit(base)
+        return 0
     cores = os.cpu_count() or 1
     total = args.warmup + args.steps
-    seconds = max(5.0, min(15.0, 150.0 / total))
+    seconds = max(2.0, min(10.0, 150.0 / total))
+    roots = fx["roots"]
+    counts = dict(zip(roots, fx["counts"]))
+    # heaviest first (longest-processing-time order), so every heavy root
+    # starts at once and the light ones fill the remaining threads
+    order = sorted(roots, key=lambda r: -counts[r])
+    light = [r for r in roots if counts[r] < LIGHT_ROOT]
     with tempfile.TemporaryDirectory() as td:
-        path = os.path.join(td, "rmat20.txt")
-        with open(path, "w") as f:
-            step = 1 << 20
-            for i in range(0, len(u), step):
-                blk = np.stack([u[i:i + step], v[i:i + step]], axis=1)
-                f.write("\n".join(f"{a} {b}" for a, b in blk.tolist()))
-                f.write("\n")
-        out = subprocess.run([REF_CPU, "steps", path, str(cores), str(seconds), str(args.warmup), str(args.steps)],
-                             capture_output=True, text=True, timeout=60 + total * (seconds + 30) + 600)
+        binp = os.path.join(td, "rmat20.bin")
+        # the ordered graph comes from a separate process (generator + oracle)
+        gen = subprocess.run([sys.executable, os.path.join(ROOT, "oracle", "ordered_bin.py"), "rmat20", binp],
+                             capture_output=True, text=True, timeout=900)
+        if gen.returncode != 0 or fx["csr_sha256"] not in gen.stdout:
+            base["unavailable"] = f"could not write the ordered graph: {(gen.stdout + gen.stderr).strip()[-200:]}"
+            emit(base)
+            return 0
+        lightf = os.path.join(td, "light.txt")
+        with open(lightf, "w") as f:
+            f.write("\n".join(map(str, light)))
+        chk = subprocess.run([REF_CPU, "edge_roots", binp, str(cores), lightf], capture_output=True, text=True,
+                             timeout=600)
+        got = {int(p[1]): int(p[2]) for p in (ln.split() for ln in chk.stdout.splitlines()) if p[:1] == ["ROOT"]}
+        bad = [r for r in light if got.get(r) != counts[r]]
+        if chk.returncode != 0 or bad:
+            raise RuntimeError(f"reference edge-root counts differ from the fixture on roots {bad[:5]}")
+        orderf = os.path.join(td, "order.txt")
+        with open(orderf, "w") as f:
+            f.write("\n".join(map(str, order)))
+        out = subprocess.run([REF_CPU, "edge_steps", binp, str(cores), orderf, str(seconds), str(args.warmup),
+                              str(args.steps)], capture_output=True, text=True,
+                             timeout=60 + total * (seconds + 30) + 600)
     steps = []
     for line in out.stdout.splitlines():
         p = line.split()
         if len(p) >= 8 and p[0] == "STEP":
             steps.append((int(p[1]), int(p[3]), float(p[5]), int(p[7])))
-    timed = [s for s in steps if s[0] >= args.warmup]
+    timed = [st for st in steps if st[0] >= args.warmup]
     if out.returncode != 0 or len(timed) != args.steps:
         base["unavailable"] = f"reference CPU run failed (exit {out.returncode}): {out.stderr.strip()[-200:]}"
         emit(base)
         return 0
-    cl = sum(s[1] for s in timed)
-    sec = sum(s[2] for s in timed)
+    cl = sum(st[1] for st in timed)
+    sec = sum(st[2] for st in timed)
     value = cl / sec
-    sample = (f"reference MceSolver::BKFixedMemPivotBit2 over vertex roots in a seeded random order, "
-              f"{seconds:.1f} s per step on {cores} threads; cliques counted by the deadline")
-    base.update({"value": value, "ms_per_step": 1000.0 * sec / len(timed),
-                 "config": {"workload": workload_name(args.sample).split(";")[0] +
-                            "; reference CPU solver, time-bounded steps", "parallelism": f"{cores} host threads"},
+    heavy = sum(1 for r in roots if counts[r] >= LIGHT_ROOT)
+    sample = (f"reference MceSolver::BKFixedMemPivotBit2 on the same {len(roots)} edge roots of the engine-ordered "
+              f"graph (.bin), heaviest first, {cores} threads, {seconds:.1f} s per step, cliques counted at the "
+              f"deadline; its {len(light)} light roots were first solved to completion and matched the fixture root "
+              f"for root.  {heavy} roots hold {sum(counts[r] for r in roots if counts[r] >= LIGHT_ROOT) / fx['count']:.2%} "
+              f"of the cliques and the reference parallelises across roots only, so at most {heavy} threads stay "
+              f"busy after the light roots")
+    base.update({"value": value, "ms_per_step": 1000.0 * sec / len(timed), "config": sample_config(fx, args.sample),
                  "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
                                   "sample": sample},
-                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                 "parity": "reference light roots == oracle fixture"})
     emit(base)
     return 0
 
 
 # ----------------------------------------------------------------- our engine
 
-def cpu_baseline(g, roots, seconds):
+def cpu_baseline(g, roots, seconds, fx=None):
     """The oracle (our C restatement of the reference's CPU path) on the host
-    cores, time-bounded, on the same graph and root sample."""
+    cores, time-bounded, on the same graph and root sample: heaviest roots
+    first when the fixture gives per-root counts, as the reference arm runs."""
     import numpy as np
 
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -225,12 +281,37 @@ def cpu_baseline(g, roots, seconds):
     ro, ci, lab = g.export_csr()
     og = oracle.Graph.from_csr(ro.astype(np.uint64), ci, lab)
     cores = os.cpu_count() or 1
-    rng = np.random.default_rng(SAMPLE_SEED)
-    order = rng.permutation(roots)
+    if fx is not None and [int(r) for r in roots] == fx["roots"]:
+        cnt = dict(zip(fx["roots"], fx["counts"]))
+        order = np.array(sorted(fx["roots"], key=lambda r: -cnt[r]), np.uint64)
+        how = "heaviest first"
+    else:
+        order = np.random.default_rng(SAMPLE_SEED).permutation(roots)
+        how = "in random order"
     res, started, el = og.mce_roots_timed(order, cores, seconds)
     return {"value": res.count / el, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"oracle over the same {len(roots)}-root sample in random order, {el:.1f} s on {cores} "
-                      f"threads ({started} roots started, {res.count} cliques)"}
+            "sample": f"oracle over the same {len(roots)}-root sample {how}, {el:.1f} s on {cores} threads "
+                      f"({started} roots started, {res.count} cliques by the deadline); it parallelises across "
+                      f"roots only, like the reference's CPU solver"}
+
+
+def check_fixture(g, r, fx):
+    """The engine's ordered graph and the sample's result against the oracle
+    fixture: CSR digest, count, checksum, histogram, largest clique."""
+    import hashlib
+
+    import numpy as np
+
+    ro, ci, lab = g.export_csr()
+    h = hashlib.sha256()
+    for a in (ro, ci, lab):
+        h.update(np.ascontiguousarray(a, dtype="<u4").tobytes())
+    if h.hexdigest() != fx["csr_sha256"]:
+        raise RuntimeError("the ordered CSR differs from the oracle fixture's")
+    got = (r.count, f"{r.checksum:016x}", {str(k): c for k, c in r.hist.items()}, r.max_size)
+    want = (fx["count"], fx["checksum"], fx["hist"], fx["max_size"])
+    if got != want:
+        raise RuntimeError(f"result differs from the oracle fixture: {got[:2]} vs {want[:2]}")
 
 
 def run_ours(args):
@@ -282,6 +363,14 @@ def run_ours(args):
     for _ in range(args.warmup):
         r, _ms = step()
         ref = (r.count, r.checksum)
+    # parity: the headline sample must reproduce the CPU oracle's fixture
+    fx = None
+    if args.workload == "rmat20-sample" and rank == 0 and os.path.exists(FIXTURE):
+        fx = load_fixture()
+        if len(fx["roots"]) != len(roots) or [int(x) for x in roots] != fx["roots"]:
+            fx = None
+        else:
+            check_fixture(g, r, fx)
     clocks = Clocks(local)
     barrier()
     torch.cuda.synchronize()
@@ -365,17 +454,22 @@ def run_ours(args):
 
     line = None
     if rank == 0:
-        cpu = cpu_baseline(g, roots, args.cpu_seconds) if world == 1 and args.cpu_seconds > 0 else None
+        cpu = cpu_baseline(g, roots, args.cpu_seconds, fx) if world == 1 and args.cpu_seconds > 0 else None
+        if fx is not None:
+            config = sample_config(fx, args.sample)
+        else:
+            config = {"workload": workload_name(args.sample, args.workload), "roots_per_step": int(len(roots)),
+                      "sample_seed": SAMPLE_SEED, "vertices": info["num_vertices"], "edges": info["num_edges"],
+                      "degeneracy": info["degeneracy"], "max_degree": info["max_degree"],
+                      "cliques_per_step": int(ref[0]), "checksum": f"{ref[1]:016x}",
+                      "l2": "512 MiB device write before every GPU step (L2 is 126 MB)",
+                      "parallelism": f"{world} rank(s), independent root samples"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": workload_name(args.sample, args.workload), "roots_per_step": int(len(roots)),
-                       "sample_seed": SAMPLE_SEED, "vertices": info["num_vertices"], "edges": info["num_edges"],
-                       "degeneracy": info["degeneracy"], "max_degree": info["max_degree"],
-                       "cliques_per_step": int(ref[0]), "checksum": f"{ref[1]:016x}",
-                       "l2": "512 MiB device write before every step (L2 is 126 MB)",
-                       "parallelism": f"{world} rank(s), independent root samples"},
+            "config": config,
+            "parity": "oracle-fixture" if fx is not None else "self-consistent across steps (no fixture)",
             "roofline": {"bound": "int", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gword-ops/s",
                          "frac": achieved / peak if peak else None, "traffic": None,
                          "note": "bitmap row word-ops of one step (ANDN+POPC per active row per node, row "

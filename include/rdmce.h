@@ -74,7 +74,10 @@ typedef struct mce_options {
   void *stream;               /* cudaStream_t to run on; NULL = the engine's own stream */
   uint32_t flags;             /* MCE_FLAG_* */
   uint32_t reg_share_bound;   /* tau inside the register tiers (<= 64 columns); 0 = 24, never above share_bound */
-  uint32_t reserved[6];
+  uint32_t slab_kib;          /* cap on each warp's scratch slab in KiB (min 16); 0 = 4096.  Roots whose
+                                 ego network does not fit are solved in a second pass with larger slabs. */
+  uint32_t heavy_warps;       /* cap on the warps of that second pass; 0 = as many as memory allows */
+  uint32_t reserved[4];
 } mce_options;
 
 #define MCE_FLAG_NO_SHARING 1u   /* disable inter-warp task sharing (the NB ablation) */
@@ -243,6 +246,12 @@ mce_status mce_server_submit(mce_server *s, const uint32_t *u, const uint32_t *v
 /* done=1 and *out filled when finished; done=0 while queued or running. */
 mce_status mce_server_poll(mce_server *s, uint64_t request_id, int *done, mce_result *out,
                            double *latency_ms);
+/* Device-clock span of a finished request's GPU work (upload, build, solve,
+ * read-back), in milliseconds since the server was created.  Spans of
+ * requests that overlap show they shared the device.  MCE_ERR_BUSY while the
+ * request is queued or running. */
+mce_status mce_server_request_span(mce_server *s, uint64_t request_id, double *device_start_ms,
+                                   double *device_end_ms);
 /* Block until every submitted request has finished. */
 mce_status mce_server_drain(mce_server *s);
 void mce_server_free(mce_server *s);

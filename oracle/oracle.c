@@ -273,13 +273,19 @@ int og_apply_order(og_graph *g, const uint32_t *order) {
   for (uint32_t i = 0; i < n; i++) off[i + 1] = off[i] + (g->off[order[i] + 1] - g->off[order[i]]);
   uint32_t *adj = (uint32_t *)malloc((2 * g->m + 1) * 4);
   uint32_t *lab = (uint32_t *)malloc(((size_t)n + 1) * 4);
+  uint64_t *fill = (uint64_t *)malloc(((size_t)n + 1) * sizeof(uint64_t));
+  memcpy(fill, off, ((size_t)n + 1) * sizeof(uint64_t));
+  /* transpose fill: new id i is appended to each neighbour's row in ascending
+   * i, so every row comes out sorted without a per-row sort */
   for (uint32_t i = 0; i < n; i++) {
     uint32_t o = order[i];
-    uint64_t d = g->off[o + 1] - g->off[o];
-    for (uint64_t k = 0; k < d; k++) adj[off[i] + k] = rev[g->adj[g->off[o] + k]];
-    qsort(adj + off[i], d, 4, cmp_u32);
+    for (uint64_t e = g->off[o]; e < g->off[o + 1]; e++) {
+      const uint32_t y = rev[g->adj[e]];
+      adj[fill[y]++] = i;
+    }
     lab[i] = g->labels[o];
   }
+  free(fill);
   free(g->off); free(g->adj); free(g->labels); free(g->root_off);
   g->off = off; g->adj = adj; g->labels = lab; g->root_off = NULL;
   free(rev);
@@ -309,6 +315,70 @@ void og_sort_degeneracy(og_graph *g) {
   og_apply_order(g, order);
   g->degeneracy = (uint32_t)k;
   free(order); free(deg);
+}
+
+/* The engine's own degeneracy order (rdmce_b200/csrc/preprocess.cu,
+ * k_peel_rounds), restated sequentially so the oracle can number roots the way
+ * the engine does.  Level k starts with a scan that claims every unclaimed
+ * vertex of residual degree <= k for the current round; each round then removes
+ * its whole frontier, and a neighbour whose residual degree falls to exactly k
+ * is claimed for the next round.  An empty round ends the level (its index is
+ * skipped); the next level is k + 1 when this one claimed anything, else the
+ * smallest surviving residual degree.  Position = (round, id), so vertices of
+ * one round keep ascending id order.  Same degeneracy value as the reference's
+ * queue (src/graph.cc:281-306); only the order inside a round differs. */
+void og_sort_gpu_rounds(og_graph *g) {
+  const uint32_t n = g->n;
+  int64_t *deg = (int64_t *)malloc(((size_t)n + 1) * sizeof(int64_t));
+  uint64_t *round = (uint64_t *)calloc((size_t)n + 1, sizeof(uint64_t)); /* 0 = unclaimed, else round + 1 */
+  uint32_t *rem = (uint32_t *)malloc(((size_t)n + 1) * 4), *rem2 = (uint32_t *)malloc(((size_t)n + 1) * 4);
+  uint32_t *fr = (uint32_t *)malloc(((size_t)n + 1) * 4), *fr2 = (uint32_t *)malloc(((size_t)n + 1) * 4);
+  for (uint32_t x = 0; x < n; x++) { deg[x] = (int64_t)(g->off[x + 1] - g->off[x]); rem[x] = x; }
+  uint64_t nrem = n, removed = 0, r = 0;
+  int64_t k = 0, degen = 0;
+  while (removed < n) {
+    uint64_t nf = 0, nsurv = 0;
+    int64_t rmin = INT64_MAX;
+    for (uint64_t i = 0; i < nrem; i++) {
+      const uint32_t v = rem[i];
+      if (round[v]) continue;
+      if (deg[v] <= k) { round[v] = r + 1; fr[nf++] = v; }
+      else { rem2[nsurv++] = v; if (deg[v] < rmin) rmin = deg[v]; }
+    }
+    uint64_t claims = 0;
+    while (nf) {
+      claims += nf;
+      removed += nf;
+      uint64_t nn = 0;
+      for (uint64_t i = 0; i < nf; i++) {
+        const uint32_t v = fr[i];
+        for (uint64_t e = g->off[v]; e < g->off[v + 1]; e++) {
+          const uint32_t u = g->adj[e];
+          if (round[u]) continue;
+          if (--deg[u] == k) { round[u] = r + 2; fr2[nn++] = u; }
+        }
+      }
+      uint32_t *t = fr; fr = fr2; fr2 = t;
+      nf = nn;
+      r++;
+    }
+    r++; /* the empty round's index is skipped */
+    { uint32_t *t = rem; rem = rem2; rem2 = t; }
+    nrem = nsurv;
+    if (claims) { degen = k; k++; }
+    else if (rmin == INT64_MAX) break;
+    else k = (k + 1 > rmin) ? k + 1 : rmin;
+  }
+  /* order = vertices by (round, id): a counting sort over rounds keeps ids ascending */
+  uint64_t *cnt = (uint64_t *)calloc(r + 2, sizeof(uint64_t));
+  for (uint32_t x = 0; x < n; x++) cnt[round[x]]++;
+  uint64_t acc = 0;
+  for (uint64_t i = 0; i < r + 2; i++) { uint64_t c = cnt[i]; cnt[i] = acc; acc += c; }
+  uint32_t *order = (uint32_t *)malloc(((size_t)n + 1) * 4);
+  for (uint32_t x = 0; x < n; x++) order[cnt[round[x]]++] = x;
+  og_apply_order(g, order);
+  g->degeneracy = (uint32_t)degen;
+  free(order); free(cnt); free(deg); free(round); free(rem); free(rem2); free(fr); free(fr2);
 }
 
 void og_core_numbers(const og_graph *g, uint32_t *core) {
@@ -716,6 +786,25 @@ int og_mce_roots(const og_graph *g, const uint64_t *roots, uint64_t nroots, int 
   return 0;
 }
 
+int og_mce_root_set(const og_graph *g, const uint64_t *roots, uint64_t nroots, int threads, uint64_t *counts,
+                    uint64_t *checksums, og_result *out) {
+  build_root_off((og_graph *)g);
+  for (uint64_t k = 0; k < nroots; k++)
+    if (roots[k] >= g->m) return -1;
+  uint64_t *cnt = counts ? counts : (uint64_t *)calloc(nroots ? nroots : 1, 8);
+  uint64_t *chk = checksums ? checksums : (uint64_t *)calloc(nroots ? nroots : 1, 8);
+  job_t J;
+  memset(&J, 0, sizeof(J));
+  J.g = g; J.begin = 0; J.end = nroots; J.roots = roots; J.counts = cnt; J.checksums = chk;
+  J.expand_r = 1;
+  run_job(&J, threads);
+  merge(out, J.partial, J.nthreads);
+  free(J.partial);
+  if (!counts) free(cnt);
+  if (!checksums) free(chk);
+  return 0;
+}
+
 int og_mce_roots_timed(const og_graph *g, const uint64_t *roots, uint64_t nroots, int threads, double seconds,
                        og_result *out, uint64_t *roots_started, double *elapsed) {
   build_root_off((og_graph *)g);
@@ -791,12 +880,14 @@ og_graph *og_load_bin(const char *path) {
 
 /* Per-root ego-network sizes: p, x before and after dropping X rows with no P
  * neighbour (include/graph_gpu.cuh:90-106).  Used to size scratch tiers. */
-void og_root_sizes(const og_graph *g, uint64_t begin, uint64_t end, uint32_t *p_out, uint32_t *x_out,
-                   uint32_t *xc_out) {
+static void root_sizes_impl(const og_graph *g, const uint64_t *list, uint64_t begin, uint64_t end, uint32_t *p_out,
+                            uint32_t *x_out, uint32_t *xc_out) {
   build_root_off((og_graph *)g);
   uint32_t *cand = NULL;
   size_t cap = 0;
-  for (uint64_t r = begin; r < end && r < g->m; r++) {
+  for (uint64_t k = begin; k < end; k++) {
+    const uint64_t r = list ? list[k] : k;
+    if (r >= g->m) break;
     uint32_t v0, v1;
     root_of(g, r, &v0, &v1);
     const uint32_t *a = g->adj + g->off[v0], *b = g->adj + g->off[v1];
@@ -822,9 +913,19 @@ void og_root_sizes(const og_graph *g, uint64_t begin, uint64_t end, uint32_t *p_
           else t++;
         }
       }
-    p_out[r - begin] = (uint32_t)p;
-    x_out[r - begin] = (uint32_t)x;
-    xc_out[r - begin] = (uint32_t)xc;
+    p_out[k - begin] = (uint32_t)p;
+    x_out[k - begin] = (uint32_t)x;
+    xc_out[k - begin] = (uint32_t)xc;
   }
   free(cand);
+}
+
+void og_root_sizes(const og_graph *g, uint64_t begin, uint64_t end, uint32_t *p_out, uint32_t *x_out,
+                   uint32_t *xc_out) {
+  root_sizes_impl(g, NULL, begin, end < g->m ? end : g->m, p_out, x_out, xc_out);
+}
+
+void og_root_sizes_list(const og_graph *g, const uint64_t *roots, uint64_t nroots, uint32_t *p_out, uint32_t *x_out,
+                        uint32_t *xc_out) {
+  root_sizes_impl(g, roots, 0, nroots, p_out, x_out, xc_out);
 }

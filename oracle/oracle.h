@@ -58,6 +58,10 @@ void og_export(const og_graph *g, uint64_t *off, uint32_t *adj, uint32_t *labels
 
 /* Degeneracy order exactly as Graph::SortByDegeneracy + ApplyOrder (src/graph.cc:281-306, 54-77). */
 void og_sort_degeneracy(og_graph *g);
+/* The engine's round-synchronous k-core peel (rdmce_b200/csrc/preprocess.cu,
+ * k_peel_rounds): position = (round, id).  Gives the engine's exact CSR, so
+ * root ids (edges v0 < v1 in CSR order) agree with the engine's. */
+void og_sort_gpu_rounds(og_graph *g);
 /* Relabel with an explicit order: new id i is old vertex order[i]. */
 int og_apply_order(og_graph *g, const uint32_t *order);
 /* Core number of every vertex (any valid peeling gives the same numbers). */
@@ -71,7 +75,10 @@ int og_mce(const og_graph *g, uint64_t begin, uint64_t end, int threads, int exp
 /* Per-root count and checksum for an explicit root list. */
 int og_mce_roots(const og_graph *g, const uint64_t *roots, uint64_t nroots, int threads,
                  uint64_t *counts, uint64_t *checksums);
-/* Write every maximal clique (original labels, ascending) as lines into a file. */
+/* The same over an explicit root list, also returning the merged result
+ * (count, checksum, histogram, largest size); counts/checksums may be NULL. */
+int og_mce_root_set(const og_graph *g, const uint64_t *roots, uint64_t nroots, int threads, uint64_t *counts,
+                    uint64_t *checksums, og_result *out);
 /* Time-bounded variant for CPU baselines: threads claim roots of the list
  * until `seconds` pass, then the search unwinds; `out` holds what was found
  * by then (count, histogram, nodes), `roots_started` the roots claimed. */
@@ -83,6 +90,10 @@ int og_list_cliques(const og_graph *g, const char *path);
 /* Per-root ego sizes p, x (all common neighbours below v1) and x after X-row compaction. */
 void og_root_sizes(const og_graph *g, uint64_t begin, uint64_t end, uint32_t *p_out, uint32_t *x_out,
                    uint32_t *xc_out);
+
+/* The same for an explicit list of root ids. */
+void og_root_sizes_list(const og_graph *g, const uint64_t *roots, uint64_t nroots, uint32_t *p_out, uint32_t *x_out,
+                        uint32_t *xc_out);
 
 /* The reference `.bin` container (src/graph.cc:154-213). */
 int og_store_bin(const og_graph *g, const char *path);

@@ -75,15 +75,19 @@ def lib():
             "og_degeneracy": (U32, [P]),
             "og_export": (None, [P, P, P, P]),
             "og_sort_degeneracy": (None, [P]),
+            "og_sort_gpu_rounds": (None, [P]),
             "og_apply_order": (I, [P, P]),
             "og_core_numbers": (None, [P, P]),
             "og_root": (None, [P, U64, C.POINTER(U32), C.POINTER(U32)]),
             "og_mce": (I, [P, U64, U64, I, I, C.POINTER(_Result)]),
             "og_mce_roots": (I, [P, P, U64, I, P, P]),
+            "og_mce_root_set": (I, [P, P, U64, I, P, P, C.POINTER(_Result)]),
             "og_mce_roots_timed": (I, [P, P, U64, I, C.c_double, C.POINTER(_Result), C.POINTER(U64),
                                        C.POINTER(C.c_double)]),
             "og_list_cliques": (I, [P, C.c_char_p]),
             "og_store_bin": (I, [P, C.c_char_p]),
+            "og_root_sizes": (None, [P, U64, U64, P, P, P]),
+            "og_root_sizes_list": (None, [P, P, U64, P, P, P]),
             "og_load_bin": (P, [C.c_char_p]),
         }
         for name, (res, args) in sig.items():
@@ -167,6 +171,12 @@ class Graph:
         lib().og_sort_degeneracy(self.h)
         return self
 
+    def sort_gpu_rounds(self):
+        """The engine's round-synchronous peel order: after this, root ids (and
+        the whole CSR) agree with the engine's for the same input."""
+        lib().og_sort_gpu_rounds(self.h)
+        return self
+
     def apply_order(self, order):
         order = np.ascontiguousarray(order, dtype=np.uint32)
         if lib().og_apply_order(self.h, _ptr(order)) != 0:
@@ -206,6 +216,20 @@ class Graph:
             raise ValueError("root id out of range")
         return cnt, chk
 
+    def mce_root_set(self, roots, threads=1):
+        """Per-root counts and checksums plus the merged result (histogram
+        included) over an explicit root list."""
+        roots = np.ascontiguousarray(roots, dtype=np.uint64)
+        cnt = np.zeros(len(roots), dtype=np.uint64)
+        chk = np.zeros(len(roots), dtype=np.uint64)
+        res = _Result()
+        if lib().og_mce_root_set(self.h, _ptr(roots), len(roots), threads, _ptr(cnt), _ptr(chk),
+                                 C.byref(res)) != 0:
+            raise ValueError("root id out of range")
+        hist = {s: int(res.hist[s]) for s in range(HIST_LEN) if res.hist[s]}
+        return cnt, chk, OracleResult(res.count, res.checksum, hist, res.max_size, res.nodes, res.pivot_words,
+                                      res.filter_rows, res.build_bytes)
+
     def mce_roots_timed(self, roots, threads, seconds):
         """Cliques found under the listed roots within `seconds` (all threads);
         returns (OracleResult so far, roots started, elapsed seconds)."""
@@ -218,6 +242,15 @@ class Graph:
         hist = {s: int(res.hist[s]) for s in range(HIST_LEN) if res.hist[s]}
         return (OracleResult(res.count, res.checksum, hist, res.max_size, res.nodes, res.pivot_words,
                              res.filter_rows, res.build_bytes), started.value, el.value)
+
+    def root_sizes_list(self, roots):
+        """Candidate-column count p of each listed root's ego network."""
+        roots = np.ascontiguousarray(roots, dtype=np.uint64)
+        p = np.zeros(len(roots), np.uint32)
+        x = np.zeros(len(roots), np.uint32)
+        xc = np.zeros(len(roots), np.uint32)
+        lib().og_root_sizes_list(self.h, _ptr(roots), len(roots), _ptr(p), _ptr(x), _ptr(xc))
+        return p
 
     def list_cliques(self, path):
         if lib().og_list_cliques(self.h, path.encode()) != 0:

@@ -18,7 +18,20 @@
 //                                    reports the cliques found so far and exits
 //   ref_cpu stats <graph>            n, m, max degree, degeneracy after the sort
 //   ref_cpu csr <graph> <out>        CSR + labels after the sort (binary dump)
-// <graph> is COO text (sorted by degeneracy as main.cc:26-27 does) or a .bin.
+//   ref_cpu storebin <graph> <out>   Graph::StoreIntoBin of the loaded (sorted) graph
+//   ref_cpu edge_roots <graph> <threads> <rootfile>
+//                                    the listed EDGE roots (ids = edges v0 < v1 in CSR
+//                                    order of the graph as loaded), each solved to
+//                                    completion by BKFixedMemPivotBit2 with R = {v0, v1},
+//                                    P = common neighbours > v1, X = the others, as the
+//                                    reference's own edge-root loop does (src/mce.cc:96-131,
+//                                    kept there as a comment); prints per-root counts
+//   ref_cpu edge_steps <graph> <threads> <rootfile> <seconds> <warmup> <steps>
+//                                    bench steps over those edge roots in file order:
+//                                    all threads until <seconds> (forked child per step,
+//                                    as `steps`), cliques counted at the deadline
+// <graph> is COO text (sorted by degeneracy as main.cc:26-27 does) or a .bin
+// (used in stored order: main.cc:26 sorts only non-.bin input).
 #include <atomic>
 #include <random>
 #include <sys/wait.h>
@@ -53,6 +66,57 @@ static void load(Graph &g, const std::string &path) {
     g.LoadFromFile(path);
     g.SortByOrder(OrderType::DEG);
   }
+}
+
+// Edge roots in CSR order: root r is the r-th pair (v0, v1), v0 < v1, walking
+// the rows in id order.  upper[v] = index of v's first root.
+struct EdgeRoots {
+  std::vector<uint64_t> upper;
+  explicit EdgeRoots(const Graph &g) {
+    const uint64_t n = g.GetNumVertices();
+    upper.assign(n + 1, 0);
+    for (uint64_t v = 0; v < n; v++) {
+      uint64_t up = 0;
+      for (vid_t w : g.N((vid_t)v)) up += w > v;
+      upper[v + 1] = upper[v] + up;
+    }
+  }
+  bool get(const Graph &g, uint64_t r, vid_t *v0, vid_t *v1) const {
+    if (r >= upper.back()) return false;
+    const uint64_t v = (uint64_t)(std::upper_bound(upper.begin(), upper.end(), r) - upper.begin()) - 1;
+    const vlist_t &row = g.N((vid_t)v);
+    const uint64_t lower = row.size() - (upper[v + 1] - upper[v]);
+    *v0 = (vid_t)v;
+    *v1 = row[lower + (r - upper[v])];
+    return true;
+  }
+};
+
+// One edge root through the reference solver, as its edge-root loop does.
+static void solve_edge_root(MceSolver &s, const Graph &g, vid_t v0, vid_t v1) {
+  vlist_t cand;
+  std::set_intersection(g.N(v0).begin(), g.N(v0).end(), g.N(v1).begin(), g.N(v1).end(), std::back_inserter(cand));
+  vlist_t R, P, X;
+  R.emplace_back(v0);
+  R.emplace_back(v1);
+  for (auto c : cand) {
+    if (c > v1) P.emplace_back(c);
+    else X.emplace_back(c);
+  }
+  if (P.empty()) {
+    if (X.empty()) s.IncrementMceCount();
+    return;
+  }
+  if (X.size() > (P.size() + 1) * 16) X = s.Partition(P, X);
+  s.BKFixedMemPivotBit2(R, P, X);
+}
+
+static std::vector<uint64_t> read_roots(const char *path) {
+  std::vector<uint64_t> roots;
+  std::ifstream f(path);
+  uint64_t r;
+  while (f >> r) roots.push_back(r);
+  return roots;
 }
 
 int main(int argc, char **argv) {
@@ -91,6 +155,99 @@ int main(int argc, char **argv) {
     }
     std::fwrite(labels.data(), 4, n, f);
     std::fclose(f);
+    return 0;
+  }
+  if (mode == "storebin") {
+    if (argc < 4) return 2;
+    g.StoreIntoBin(argv[3]);  // writes <argv[3] without its extension>.bin
+    return 0;
+  }
+  if (mode == "edge_roots" || mode == "edge_steps") {
+    if (argc < 5) return 2;
+    const int threads = std::max(1, std::atoi(argv[3]));
+    const std::vector<uint64_t> roots = read_roots(argv[4]);
+    const EdgeRoots er(g);
+    for (uint64_t r : roots) {
+      vid_t a, b;
+      if (!er.get(g, r, &a, &b)) {
+        std::fprintf(stderr, "root %llu out of range\n", (unsigned long long)r);
+        return 1;
+      }
+    }
+    const uint64_t nr = roots.size();
+    if (mode == "edge_roots") {
+      std::vector<uint64_t> counts(nr, 0);
+      std::atomic<uint64_t> next(0);
+      auto t0 = std::chrono::steady_clock::now();
+      std::vector<std::thread> th;
+      for (int t = 0; t < threads; t++) {
+        th.emplace_back([&]() {
+          MceSolver s(g);
+          for (;;) {
+            const uint64_t k = next.fetch_add(1);
+            if (k >= nr) break;
+            vid_t v0, v1;
+            er.get(g, roots[k], &v0, &v1);
+            const acc_t c0 = s.mce_count_;
+            solve_edge_root(s, g, v0, v1);
+            counts[k] = s.mce_count_ - c0;
+          }
+        });
+      }
+      for (auto &x : th) x.join();
+      double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      uint64_t total = 0;
+      for (uint64_t k = 0; k < nr; k++) {
+        std::printf("ROOT %llu %llu\n", (unsigned long long)roots[k], (unsigned long long)counts[k]);
+        total += counts[k];
+      }
+      std::printf("RESULT count %llu seconds %.6f threads %d roots %llu\n", (unsigned long long)total, sec, threads,
+                  (unsigned long long)nr);
+      return 0;
+    }
+    if (argc < 8) return 2;
+    const double seconds = std::atof(argv[5]);
+    const int total_steps = std::atoi(argv[6]) + std::atoi(argv[7]);
+    for (int step = 0; step < total_steps; step++) {
+      std::fflush(stdout);
+      pid_t pid = fork();
+      if (pid < 0) return 1;
+      if (pid == 0) {
+        // one edge root can take far longer than a step: threads are detached
+        // and the child reports the cliques counted by the deadline, then exits
+        std::atomic<uint64_t> next(0), done(0);
+        std::vector<std::unique_ptr<MceSolver>> solvers;
+        for (int t = 0; t < threads; t++) solvers.emplace_back(new MceSolver(g));
+        auto t0 = std::chrono::steady_clock::now();
+        for (int t = 0; t < threads; t++) {
+          std::thread([&, t]() {
+            MceSolver &s = *solvers[t];
+            for (;;) {
+              const uint64_t k = next.fetch_add(1);
+              if (k >= nr) break;
+              vid_t v0, v1;
+              er.get(g, roots[k], &v0, &v1);
+              solve_edge_root(s, g, v0, v1);
+              done.fetch_add(1);
+            }
+          }).detach();
+        }
+        for (;;) {
+          std::this_thread::sleep_for(std::chrono::milliseconds(20));
+          double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+          if (el >= seconds || done.load() >= nr) {
+            uint64_t total = 0;
+            for (auto &sv : solvers) total += *(volatile acc_t *)&sv->mce_count_;
+            std::printf("STEP %d cliques %llu seconds %.6f roots_done %llu of %llu\n", step,
+                        (unsigned long long)total, el, (unsigned long long)done.load(), (unsigned long long)nr);
+            std::fflush(stdout);
+            _exit(0);
+          }
+        }
+      }
+      int status = 0;
+      waitpid(pid, &status, 0);
+    }
     return 0;
   }
   if (mode == "count" || mode == "pivot") {

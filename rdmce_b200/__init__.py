@@ -54,7 +54,9 @@ class Options(C.Structure):
         ("stream", C.c_void_p),
         ("flags", C.c_uint32),
         ("reg_share_bound", C.c_uint32),
-        ("reserved", C.c_uint32 * 6),
+        ("slab_kib", C.c_uint32),
+        ("heavy_warps", C.c_uint32),
+        ("reserved", C.c_uint32 * 4),
     ]
 
 
@@ -169,6 +171,7 @@ _SIGS = {
     "mce_server_submit": (_I, [_P, _P, _P, _U64, C.POINTER(_U64)]),
     "mce_server_poll": (_I, [_P, _U64, C.POINTER(_I), C.POINTER(_Result), C.POINTER(_D)]),
     "mce_server_drain": (_I, [_P]),
+    "mce_server_request_span": (_I, [_P, C.c_uint64, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "mce_server_free": (None, [_P]),
     "mce_mix64": (_U64, [_U64]),
     "mce_gen_rmat": (_I, [_U32, _U32, _D, _D, _D, _U64, _P, _P, _U64, C.POINTER(_U64), _I]),
@@ -480,6 +483,13 @@ class Server:
             return None
         _check(s, "request")
         return Result._from(r), lat.value
+
+    def span(self, rid: int):
+        """(start, end) of a finished request's device work, ms on the device
+        clock since the server was created."""
+        a, b = C.c_double(), C.c_double()
+        _check(lib().mce_server_request_span(self.h, rid, C.byref(a), C.byref(b)), "mce_server_request_span")
+        return a.value, b.value
 
     def drain(self):
         _check(lib().mce_server_drain(self.h), "mce_server_drain")

@@ -321,16 +321,7 @@ static mce_status solve_impl(mce_graph *g, const mce_options &o, mce_result *out
   char *res = (char *)scr->get(0, res_bytes, &s);
   if (!res) return s;
   MCE_CUDA_TRY(cudaMemsetAsync(res, 0, res_bytes, st));
-  EnumConfig cfg;
-  cfg.warps_per_block = o.warps_per_block;
-  cfg.blocks_per_sm = o.blocks_per_sm;
-  cfg.share_bound = o.share_bound ? o.share_bound : 24;
-  cfg.reg_share_bound = o.reg_share_bound;
-  cfg.expand_r = o.expand_r;
-  cfg.sharing = (o.flags & MCE_FLAG_NO_SHARING) ? 0 : 1;
-  cfg.stats = (o.flags & MCE_FLAG_STATS) ? 1 : 0;
-  cfg.root_begin = o.root_begin;
-  cfg.root_end = o.root_end;
+  EnumConfig cfg = config_from_options(o);
   cfg.spin_limit = spin_of(o);
   cfg.root_list = roots_d;
   cfg.n_root_list = n_roots;
@@ -380,6 +371,7 @@ mce_status mce_solve(mce_graph *g, const mce_options *opt, mce_result *out) {
 mce_status mce_solve_roots(mce_graph *g, const uint64_t *roots, uint64_t n_roots, const mce_options *opt,
                            uint64_t *counts, uint64_t *checksums) {
   if (!g || (n_roots && (!roots || !counts || !checksums))) return MCE_ERR_INVALID_ARG;
+  if (n_roots >= (1ULL << 32)) return MCE_ERR_INVALID_ARG;
   for (uint64_t i = 0; i < n_roots; i++)
     if (roots[i] >= g->g.m) return MCE_ERR_INVALID_ARG;
   if (!n_roots) return MCE_OK;
@@ -420,6 +412,7 @@ mce_status mce_solve_roots(mce_graph *g, const uint64_t *roots, uint64_t n_roots
 mce_status mce_solve_root_list(mce_graph *g, const uint64_t *roots, uint64_t n_roots, const mce_options *opt,
                                mce_result *out) {
   if (!g || !out || (n_roots && !roots)) return MCE_ERR_INVALID_ARG;
+  if (n_roots >= (1ULL << 32)) return MCE_ERR_INVALID_ARG;
   for (uint64_t i = 0; i < n_roots; i++)
     if (roots[i] >= g->g.m) return MCE_ERR_INVALID_ARG;
   mce_options tmp;

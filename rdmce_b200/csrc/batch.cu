@@ -26,7 +26,7 @@ struct mce_batch {
   mce::Scratch scr;
   // captured launch
   cudaGraphExec_t exec = nullptr;
-  uint32_t exec_hist_len = 0;
+  mce::EnumConfig exec_cfg;  // the settings the captured launch was planned with
   mce::EnumPlan plan;
   mce::SlotResult *slots_h = nullptr;  // pinned
   unsigned long long *hist_h = nullptr;
@@ -216,7 +216,13 @@ mce_status mce_batch_solve(mce_batch *b, const mce_options *opt, mce_batch_graph
   if (!res) return s;
   SlotResult *slots = (SlotResult *)res;
   unsigned long long *hd = (unsigned long long *)(res + slot_bytes);
-  const bool rebuild = !b->exec || b->exec_hist_len != hl;
+  // the captured launch bakes in the plan: capture again when any option
+  // that feeds the plan differs from the captured one's
+  EnumConfig cfg = config_from_options(o);
+  cfg.root_begin = cfg.root_end = 0;
+  cfg.n_slots = ng;
+  cfg.hist_len = hl;
+  const bool rebuild = !b->exec || !same_plan_settings(cfg, b->exec_cfg);
   if (rebuild) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     b->exec = nullptr;
@@ -226,13 +232,6 @@ mce_status mce_batch_solve(mce_batch *b, const mce_options *opt, mce_batch_graph
     b->hist_h = nullptr;
     MCE_CUDA_TRY(cudaMallocHost(&b->slots_h, slot_bytes));
     MCE_CUDA_TRY(cudaMallocHost(&b->hist_h, hist_bytes));
-    EnumConfig cfg;
-    cfg.warps_per_block = o.warps_per_block;
-    cfg.blocks_per_sm = o.blocks_per_sm;
-    cfg.expand_r = o.expand_r;
-    cfg.spin_limit = o.spin_limit;
-    cfg.n_slots = ng;
-    cfg.hist_len = hl;
     MCE_TRY(enum_plan(b->g, cfg, &b->scr, slots, hd, &b->plan));
     // capture: clear results, run the persistent kernel, copy results out
     cudaGraph_t graph = nullptr;
@@ -253,7 +252,7 @@ mce_status mce_batch_solve(mce_batch *b, const mce_options *opt, mce_batch_graph
       b->exec = nullptr;
       return MCE_ERR_CUDA;
     }
-    b->exec_hist_len = hl;
+    b->exec_cfg = cfg;
   }
   cudaEvent_t e0, e1;
   MCE_CUDA_TRY(cudaEventCreate(&e0));

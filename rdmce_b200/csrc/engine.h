@@ -56,7 +56,37 @@ struct EnumConfig {
   uint32_t n_slots = 1;
   uint32_t hist_len = MCE_HIST_LEN;
   uint32_t max_blocks = 0;  // cap on the grid (0 = whole GPU); the server shares the GPU
+  uint32_t slab_kib = 0;    // cap on the per-warp slab in KiB (0 = 4096)
+  uint32_t heavy_warps = 0; // cap on the large-scratch pass's warps (0 = as memory allows)
 };
+
+// The enumeration settings a caller's options select (every entry point maps
+// mce_options through this one function).
+inline EnumConfig config_from_options(const mce_options &o) {
+  EnumConfig c;
+  c.warps_per_block = o.warps_per_block;
+  c.blocks_per_sm = o.blocks_per_sm;
+  c.share_bound = o.share_bound ? o.share_bound : 24;
+  c.reg_share_bound = o.reg_share_bound;
+  c.expand_r = o.expand_r;
+  c.sharing = (o.flags & MCE_FLAG_NO_SHARING) ? 0 : 1;
+  c.stats = (o.flags & MCE_FLAG_STATS) ? 1 : 0;
+  c.root_begin = o.root_begin;
+  c.root_end = o.root_end;
+  c.spin_limit = o.spin_limit ? o.spin_limit : (1ULL << 34);
+  c.slab_kib = o.slab_kib;
+  c.heavy_warps = o.heavy_warps;
+  return c;
+}
+
+// True when two configs would produce the same launch plan (a captured
+// launch can be replayed for the second).
+inline bool same_plan_settings(const EnumConfig &a, const EnumConfig &b) {
+  return a.warps_per_block == b.warps_per_block && a.blocks_per_sm == b.blocks_per_sm &&
+         a.share_bound == b.share_bound && a.reg_share_bound == b.reg_share_bound && a.expand_r == b.expand_r &&
+         a.sharing == b.sharing && a.stats == b.stats && a.spin_limit == b.spin_limit && a.slab_kib == b.slab_kib &&
+         a.heavy_warps == b.heavy_warps && a.hist_len == b.hist_len && a.n_slots == b.n_slots;
+}
 
 struct EnumStats {
   uint64_t roots = 0;
@@ -84,13 +114,15 @@ struct Scratch;
 struct EnumParams {
   DevGraph g;
   uint64_t rb, re;                       // root range [rb, re) (range mode)
-  const uint32_t *heavy_list;            // heavy pass: root ids
-  const uint64_t *root_list;             // per-root mode: root ids
-  uint64_t n_list;                       // entries in whichever list is used
+  const uint32_t *heavy_list;            // large-scratch pass: work indices of the deferred roots
+  uint64_t n_heavy;                      // entries in heavy_list
+  const uint64_t *root_list;             // list mode: root ids (else the range [rb, re))
+  uint64_t n_list;                       // entries in root_list
   unsigned long long *next;              // claim counter
   char *slab;
   uint64_t slab_bytes;                   // per warp
-  uint32_t *heavy_out;                   // range mode: deferred roots
+  uint32_t *heavy_out;                   // deferred roots' work indices (heavy_cap entries)
+  uint32_t heavy_cap;
   unsigned int *heavy_n;
   unsigned long long *heavy_need;
   int push_heavy;
@@ -134,6 +166,7 @@ struct EnumPlan {
   uint64_t nwarps = 0, nwork = 0;
   bool fits_all = false;  // every root fits the normal slab: no deferred pass possible
   uint32_t pool_blocks = 0;
+  uint32_t heavy_warps = 0;  // cap on the large-scratch pass (0 = as memory allows)
   void *ctl = nullptr;
   Scratch *scr = nullptr;
 };

@@ -153,6 +153,23 @@ struct T1Area {
 constexpr uint32_t kT1Area = (sizeof(T1Area) + 255) & ~255u;
 constexpr uint32_t kTail = kLocalRec + kT1Area;  // slab bytes reserved at its end
 
+// Slab layout of a general-tier problem (bytes from the slab start).
+struct Layout {
+  uint64_t colv_off, hash_off, rows_off, stack_off, alist_off, need;
+};
+
+__host__ __device__ __forceinline__ Layout layout_for(uint64_t cand_n, uint32_t pc, uint32_t nrows, uint32_t W) {
+  Layout L;
+  L.colv_off = 0;
+  L.hash_off = align8(4ULL * cand_n);
+  L.rows_off = L.hash_off + 16ULL * pc;
+  L.stack_off = L.rows_off + 8ULL * (uint64_t)nrows * W;
+  // pc + 1 levels, one scratch record past the deepest, one spare
+  L.alist_off = L.stack_off + 8ULL * (uint64_t)(pc + 3) * (3ULL * W + 4);
+  L.need = L.alist_off + 4ULL * nrows + kTail;
+  return L;
+}
+
 struct Ctx {
   const EnumParams *P;
   WarpSmem *sm;
@@ -1132,9 +1149,11 @@ __device__ void reg_from_local(const Ctx &c, const char *rec) {
 // Child of candidate q at a general-tier level (record rec_l) as a task
 // record in `out`: columns = Pbase & row(q), rows = active rows holding bit q
 // (and all of R' when the level's list is inherited), compressed to the child
-// columns.  Returns false when the record would exceed max_bytes.
+// columns.  Returns false when the record would exceed max_bytes, or, for a
+// pool record (to_pool), when a warp's slab could not lay it out for the
+// general tier.
 __device__ bool gen_materialize(const Ctx &c, const Gen &G, const uint64_t *rec_l, uint32_t q,
-                                const uint64_t *Pbase, uint64_t max_bytes, char *out) {
+                                const uint64_t *Pbase, uint64_t max_bytes, bool to_pool, char *out) {
   const uint32_t lane = c.lane, W = G.W;
   if (W > 64) return false;  // the child's column mask lives in rowbuf (64 words)
   uint64_t *CP = c.sm->rowbuf;
@@ -1183,6 +1202,7 @@ __device__ bool gen_materialize(const Ctx &c, const Gen &G, const uint64_t *rec_
   }
   const uint32_t nrows = pc + nx;
   if (task_bytes(pc, nrows, Wn) > max_bytes) return false;
+  if (to_pool && layout_for(pc, pc, nrows, Wn).need > c.slab_bytes) return false;
   uint32_t *colv = (uint32_t *)(out + kHdr);
   uint64_t *rows = (uint64_t *)(out + kHdr + align8(4ULL * pc));
   // child columns: parent candidate rows i < pc with CP bit i, in order
@@ -1256,7 +1276,7 @@ __device__ bool gen_spawn(const Ctx &c, const Gen &G, int level) {
         Pbase[w] = Pl[w] & ~(VPl[w] & below);
       }
       __syncwarp();
-      const bool ok = gen_materialize(c, G, rec, q, Pbase, c.P->block_bytes, pool_block(*c.P, blk));
+      const bool ok = gen_materialize(c, G, rec, q, Pbase, c.P->block_bytes, true, pool_block(*c.P, blk));
       if (!ok) {
         pool_free(c, blk);
         return spawned > 0;
@@ -1429,7 +1449,7 @@ __device__ __noinline__ void gen_solve_body(Ctx c, Gen G, uint32_t rsize0, uint6
         }
         ccount += __popc(__ballot_sync(kFull, keep));
       }
-      if (ccount <= kT1Rows && gen_materialize(c, G, rec, q, Pv, kLocalRec, local)) {
+      if (ccount <= kT1Rows && gen_materialize(c, G, rec, q, Pv, kLocalRec, false, local)) {
         if (lane == 0) sm->gen_level = level;
         __syncwarp();
         const unsigned long long t0 = now(), sp0 = sm->cyc[kCycSpawn];
@@ -1617,6 +1637,32 @@ __device__ uint32_t intersect(const DevGraph &g, uint32_t v0, uint32_t v1, uint3
   return nc;
 }
 
+// |N(v0) & N(v1)| and how many of those lie below v1, without storing them:
+// sizes the large-scratch pass for a root whose ego network overflowed the slab.
+__device__ void intersect_count(const DevGraph &g, uint32_t v0, uint32_t v1, uint32_t *nc_out, uint32_t *nx_out) {
+  const uint32_t lane = lane_id();
+  const uint32_t *a = g.adj + g.off[v0], *b = g.adj + g.off[v1];
+  uint32_t da = g.off[v0 + 1] - g.off[v0], db = g.off[v1 + 1] - g.off[v1];
+  if (da > db) {
+    const uint32_t *t = a;
+    a = b;
+    b = t;
+    const uint32_t td = da;
+    da = db;
+    db = td;
+  }
+  uint32_t nc = 0, nx = 0;
+  for (uint32_t base = 0; base < da; base += 32) {
+    const uint32_t t = base + lane;
+    const uint32_t val = t < da ? __ldg(a + t) : 0;
+    const bool hit = t < da && contains_u32(b, db, val);
+    nc += __popc(__ballot_sync(kFull, hit));
+    nx += __popc(__ballot_sync(kFull, hit && val < v1));
+  }
+  *nc_out = nc;
+  *nx_out = nx;
+}
+
 // Ego bitmap rows (candidate rows, then X rows with a candidate neighbour).
 __device__ uint32_t build_rows(const DevGraph &g, const uint32_t *cand, uint32_t x, uint32_t p, uint32_t W,
                                uint64_t *rows, uint64_t *rowbuf) {
@@ -1676,23 +1722,6 @@ __device__ uint32_t build_rows(const DevGraph &g, const uint32_t *cand, uint32_t
     if (r < p || any) nrows++;
   }
   return nrows;
-}
-
-// Slab layout of a general-tier problem (bytes from the slab start).
-struct Layout {
-  uint64_t colv_off, hash_off, rows_off, stack_off, alist_off, need;
-};
-
-__host__ __device__ __forceinline__ Layout layout_for(uint64_t cand_n, uint32_t pc, uint32_t nrows, uint32_t W) {
-  Layout L;
-  L.colv_off = 0;
-  L.hash_off = align8(4ULL * cand_n);
-  L.rows_off = L.hash_off + 16ULL * pc;
-  L.stack_off = L.rows_off + 8ULL * (uint64_t)nrows * W;
-  // pc + 1 levels, one scratch record past the deepest, one spare
-  L.alist_off = L.stack_off + 8ULL * (uint64_t)(pc + 3) * (3ULL * W + 4);
-  L.need = L.alist_off + 4ULL * nrows + kTail;
-  return L;
 }
 
 // Solve root r.  Returns false when the root does not fit this slab.
@@ -1859,8 +1888,7 @@ __global__ void __launch_bounds__(256, 4) k_enumerate(const __grid_constant__ En
   c.slab_bytes = P.slab_bytes;
   c.ta = (T1Area *)(c.slab + c.slab_bytes - kTail);
   c.sharing = P.sharing != 0;
-  const bool range_mode = P.heavy_list == nullptr && P.root_list == nullptr;
-  const uint64_t total = range_mode ? P.re - P.rb : P.n_list;
+  const uint64_t total = P.heavy_list ? P.n_heavy : (P.root_list ? P.n_list : P.re - P.rb);
   unsigned long long nroots = 0;
   bool roots_left = true;
   uint64_t idle_spins = 0;
@@ -1891,22 +1919,32 @@ __global__ void __launch_bounds__(256, 4) k_enumerate(const __grid_constant__ En
       if (c.lane == 0) k = atomicAdd(P.next, 1ULL);
       k = __shfl_sync(kFull, k, 0);
       if (k < total) {
-        uint64_t r;
-        if (P.heavy_list) r = P.heavy_list[k];
-        else if (P.root_list) r = P.root_list[k];
-        else r = P.re - 1 - k;  // late-peeled roots first
+        // wk: the root's index in this solve's work list (per-root results are
+        // kept by it); the large-scratch pass walks a list of such indices
+        const uint64_t wk = P.heavy_list ? P.heavy_list[k] : k;
+        const uint64_t r = P.root_list ? P.root_list[wk] : P.re - 1 - wk;  // range: late-peeled roots first
         const unsigned long long c0 = sm->count, h0 = sm->checksum;
         nroots++;
         const unsigned long long tr = now();
         const bool fit = solve_root(c, r);
         if (c.lane == 0) atomicMax(P.stat_max_item, now() - tr);
-        if (!fit && c.lane == 0) {
+        if (!fit) {
           if (P.push_heavy) {
-            P.heavy_out[atomicAdd(P.heavy_n, 1u)] = (uint32_t)r;
-            const uint32_t v0 = P.g.root_v0[r], v1 = P.g.root_v1[r];
-            const uint32_t dmin = min(P.g.off[v0 + 1] - P.g.off[v0], P.g.off[v1 + 1] - P.g.off[v1]);
-            atomicMax(P.heavy_need, (unsigned long long)layout_for(dmin, dmin, dmin, (dmin + 63) / 64).need);
-          } else {
+            // defer the root, sized exactly: the slab must hold its candidate
+            // list and an ego network of p columns and up to nc rows
+            uint32_t nc = 0, nx = 0;
+            intersect_count(P.g, P.g.root_v0[r], P.g.root_v1[r], &nc, &nx);
+            if (c.lane == 0) {
+              const uint32_t slot = atomicAdd(P.heavy_n, 1u);
+              if (slot < P.heavy_cap) {
+                P.heavy_out[slot] = (uint32_t)wk;
+                const uint32_t p = nc - nx;
+                atomicMax(P.heavy_need, (unsigned long long)layout_for(nc, p, nc, (p + 63) / 64).need);
+              } else {
+                atomicExch(P.error, 4u);  // more deferred roots than the list holds
+              }
+            }
+          } else if (c.lane == 0) {
             atomicExch(P.error, 2u);
           }
         }
@@ -1917,8 +1955,10 @@ __global__ void __launch_bounds__(256, 4) k_enumerate(const __grid_constant__ En
           __syncwarp();
           if (c.lane == 0) {
             sm->checksum += lc;
-            P.per_root_count[k] = fit ? sm->count - c0 : ~0ULL;
-            P.per_root_checksum[k] = sm->checksum - h0;
+            if (fit) {  // a deferred root's values come from the large-scratch pass
+              P.per_root_count[wk] = sm->count - c0;
+              P.per_root_checksum[wk] = sm->checksum - h0;
+            }
           }
         }
         __syncwarp();
@@ -2127,17 +2167,20 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
   const uint64_t dcap = std::max<uint32_t>(1, g.max_degree);
   const Layout LB = layout_for(dcap, (uint32_t)kcap, (uint32_t)(kcap + dcap), (uint32_t)((kcap + 63) / 64));
   const uint64_t bound = align8(LB.need + 3ULL * (kcap + dcap) * 4);
-  uint64_t slab_bytes = std::max<uint64_t>(std::min<uint64_t>(bound, 4ULL << 20), 16ULL << 10);
+  const uint64_t slab_cap = cfg.slab_kib ? std::max<uint64_t>(16, cfg.slab_kib) << 10 : 4ULL << 20;
+  uint64_t slab_bytes = std::max<uint64_t>(std::min<uint64_t>(bound, slab_cap), 16ULL << 10);
   while (slab_bytes > (64ULL << 10) && slab_bytes * nwarps > freeb / 2) slab_bytes >>= 1;
   slab_bytes = (slab_bytes + 255) & ~255ULL;  // every warp's slab (and its T1Area) 256-byte aligned
   plan->fits_all = slab_bytes >= bound;
   char *slab = (char *)scr->get(2, slab_bytes * nwarps, &s);
   if (!slab) return s;
-  // deferred roots need a list unless per-root counts are being attributed
-  const bool defer = cfg.per_root_count == nullptr;
+  // roots whose ego network overflows the slab are deferred to a second pass;
+  // the list holds their work indices (a solve of more than 2^32 roots is
+  // refused by the callers)
+  const uint64_t heavy_cap = std::min<uint64_t>(nwork, 1ULL << 26);
   uint32_t *heavy = nullptr;
-  if (defer && nwork) {
-    heavy = (uint32_t *)scr->get(3, nwork * 4, &s);
+  if (nwork) {
+    heavy = (uint32_t *)scr->get(3, heavy_cap * 4, &s);
     if (!heavy) return s;
   }
   // task pool: one record per block; both rings have one cell per block
@@ -2164,7 +2207,9 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
   P.root_list = list_mode ? cfg.root_list : nullptr;
   P.n_list = list_mode ? cfg.n_root_list : 0;
   P.heavy_out = heavy;
-  P.push_heavy = defer ? 1 : 0;
+  P.heavy_cap = (uint32_t)heavy_cap;
+  P.push_heavy = 1;
+  plan->heavy_warps = cfg.heavy_warps;
   plan->blocks = blocks;
   plan->threads = wpb * 32;
   plan->smem = (size_t)wpb * sizeof(WarpSmem);
@@ -2199,25 +2244,36 @@ mce_status enum_finish(const EnumPlan &plan, cudaStream_t st, EnumStats *stats) 
   uint64_t max_item[2] = {h.stat_max_item[0], h.stat_max_item[1]};
   uint32_t err = h.error;
   if (h.heavy_n && !h.error) {
-    // deferred roots: large slabs, and every warp of the pass shares their work
+    // Deferred roots: one slab per warp, each sized for the largest deferred
+    // ego network; every warp of the pass shares their work (unless per-root
+    // values are being attributed, which keeps each root on one warp).  Only
+    // warps that get a slab are launched: with fewer slabs than a block's
+    // warps, the block shrinks to that many.
     size_t freeb = 0, totalb = 0;
     MCE_CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
     const uint64_t need = ((h.heavy_need + 4096) + 255) & ~255ULL;
-    const uint64_t hw = std::min<uint64_t>((uint64_t)(freeb * 0.7) / need, plan.nwarps);
+    uint64_t hw = std::min<uint64_t>((uint64_t)(freeb * 0.7) / need, plan.nwarps);
+    if (plan.heavy_warps) hw = std::min<uint64_t>(hw, plan.heavy_warps);
+    hw = std::min<uint64_t>(hw, h.heavy_n);
     if (hw == 0) return MCE_ERR_OUT_OF_MEMORY;
-    mce_status s = MCE_OK;
-    char *big = (char *)plan.scr->get(4, need * hw, &s);
-    if (!big) return s;
     EnumPlan H = plan;
+    const uint32_t wpb = plan.threads / 32;
+    if (hw < wpb) {
+      H.blocks = 1;
+      H.threads = (uint32_t)hw * 32;
+      H.smem = (size_t)hw * sizeof(WarpSmem);
+    } else {
+      H.blocks = (uint32_t)(hw / wpb);
+    }
+    H.nwarps = (uint64_t)H.blocks * (H.threads / 32);
+    mce_status s = MCE_OK;
+    char *big = (char *)plan.scr->get(4, need * H.nwarps, &s);
+    if (!big) return s;
     H.params.slab = big;
     H.params.slab_bytes = need;
     H.params.heavy_list = plan.params.heavy_out;
-    H.params.root_list = nullptr;
-    H.params.n_list = h.heavy_n;
+    H.params.n_heavy = h.heavy_n;
     H.params.push_heavy = 0;
-    const uint32_t wpb = plan.threads / 32;
-    H.blocks = (uint32_t)std::max<uint64_t>(1, hw / wpb);
-    H.nwarps = (uint64_t)H.blocks * wpb;
     H.params.nwarps = (uint32_t)H.nwarps;
     MCE_TRY(reset_ctl(H, st));
     k_enumerate<<<H.blocks, H.threads, H.smem, st>>>(H.params);
@@ -2247,6 +2303,7 @@ mce_status enum_finish(const EnumPlan &plan, cudaStream_t st, EnumStats *stats) 
     stats->launches = launches;
   }
   if (err == 2) return MCE_ERR_OUT_OF_MEMORY;
+  if (err == 4) return MCE_ERR_CAPACITY;
   if (err) return MCE_ERR_TIMEOUT;
   return MCE_OK;
 }

@@ -35,6 +35,7 @@ struct Request {
   mce_status status = MCE_OK;
   std::unique_ptr<mce_result> result;
   Clock::time_point t_submit, t_done;
+  double dev_start_ms = -1, dev_end_ms = -1;  // device clock, from the server's base event
 };
 
 }  // namespace
@@ -50,6 +51,9 @@ struct mce_server {
   uint32_t running = 0;
   bool stop = false;
   int sms = 148;
+  // recorded (and completed) at creation: request spans are measured from it
+  // on the device's own clock
+  cudaEvent_t base = nullptr;
 };
 
 namespace mce {
@@ -68,19 +72,24 @@ uint64_t estimate_bytes(const Request &r) {
 void run_request(mce_server *s, Request *r, cudaStream_t st, Scratch *scr) {
   DeviceGraph g;
   mce_status rc = MCE_OK;
-  uint32_t *ud = nullptr, *vd = nullptr;
   const uint64_t np = r->u.size();
   const size_t bytes = std::max<uint64_t>(np, 1) * 4;
   auto t0 = Clock::now();
-  if (cudaMallocAsync(&ud, bytes, st) != cudaSuccess || cudaMallocAsync(&vd, bytes, st) != cudaSuccess)
-    rc = MCE_ERR_OUT_OF_MEMORY;
+  // the request's device span: from before its upload to after its results
+  // are read back, on the worker's stream
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (cudaEventCreate(&ev0) != cudaSuccess || cudaEventCreate(&ev1) != cudaSuccess) rc = MCE_ERR_CUDA;
+  if (ev0) cudaEventRecord(ev0, st);
+  // the request's pairs go to the worker's kept scratch (grown on demand and
+  // reused by later requests), so a request of a size seen before allocates
+  // nothing here
+  uint32_t *ud = (uint32_t *)scr->get(7, 2 * bytes, &rc);
+  uint32_t *vd = ud ? ud + bytes / 4 : nullptr;
   if (rc == MCE_OK && np &&
       (cudaMemcpyAsync(ud, r->u.data(), np * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
        cudaMemcpyAsync(vd, r->v.data(), np * 4, cudaMemcpyHostToDevice, st) != cudaSuccess))
     rc = MCE_ERR_CUDA;
   if (rc == MCE_OK) rc = build_from_pairs(ud, vd, np, MCE_ORDER_DEGENERACY, 1ULL << 34, st, &g);
-  if (ud) cudaFreeAsync(ud, st);
-  if (vd) cudaFreeAsync(vd, st);
   auto t1 = Clock::now();
   std::unique_ptr<mce_result> res(new mce_result());
   std::memset(res.get(), 0, sizeof(mce_result));
@@ -119,9 +128,20 @@ void run_request(mce_server *s, Request *r, cudaStream_t st, Scratch *scr) {
   res->degeneracy = g.degeneracy;
   res->phase_ms[MCE_PHASE_PREPROCESS] = std::chrono::duration<double, std::milli>(t1 - t0).count();
   free_graph(&g);
+  float span0 = -1, span1 = -1;
+  if (ev1) {
+    cudaEventRecord(ev1, st);
+    if (cudaEventSynchronize(ev1) != cudaSuccess || cudaEventElapsedTime(&span0, s->base, ev0) != cudaSuccess ||
+        cudaEventElapsedTime(&span1, s->base, ev1) != cudaSuccess)
+      span0 = span1 = -1;
+  }
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
   cudaStreamSynchronize(st);
   cudaGetLastError();
   std::lock_guard<std::mutex> lk(s->mu);
+  r->dev_start_ms = span0;
+  r->dev_end_ms = span1;
   r->status = rc;
   r->result = std::move(res);
   r->t_done = Clock::now();
@@ -203,6 +223,12 @@ mce_status mce_server_create(const mce_server_options *opt, mce_server **out) {
   if (!s) return MCE_ERR_OUT_OF_MEMORY;
   s->opt = o;
   s->budget = o.memory_budget ? o.memory_budget : (uint64_t)(freeb * 0.6);
+  if (cudaEventCreate(&s->base) != cudaSuccess || cudaEventRecord(s->base, 0) != cudaSuccess ||
+      cudaEventSynchronize(s->base) != cudaSuccess) {
+    if (s->base) cudaEventDestroy(s->base);
+    delete s;
+    return MCE_ERR_CUDA;
+  }
   cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, o.device);
   for (uint32_t i = 0; i < o.max_inflight; i++) s->workers.emplace_back(mce::worker_main, s);
   *out = s;
@@ -243,6 +269,19 @@ mce_status mce_server_poll(mce_server *s, uint64_t request_id, int *done, mce_re
   return r->status;
 }
 
+mce_status mce_server_request_span(mce_server *s, uint64_t request_id, double *device_start_ms,
+                                   double *device_end_ms) {
+  if (!s || !device_start_ms || !device_end_ms) return MCE_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->all.find(request_id);
+  if (it == s->all.end()) return MCE_ERR_NOT_FOUND;
+  const Request *r = it->second.get();
+  if (r->state != 2) return MCE_ERR_BUSY;
+  *device_start_ms = r->dev_start_ms;
+  *device_end_ms = r->dev_end_ms;
+  return r->dev_start_ms < 0 ? MCE_ERR_CUDA : MCE_OK;
+}
+
 mce_status mce_server_drain(mce_server *s) {
   if (!s) return MCE_ERR_INVALID_ARG;
   std::unique_lock<std::mutex> lk(s->mu);
@@ -258,6 +297,10 @@ void mce_server_free(mce_server *s) {
   }
   s->cv_work.notify_all();
   for (auto &t : s->workers) t.join();
+  if (s->base) {
+    cudaSetDevice(s->opt.device);
+    cudaEventDestroy(s->base);
+  }
   delete s;
 }
 

@@ -71,6 +71,7 @@ def test_server_results_alone_and_in_the_mix(gpu):
             time.sleep(0.002)  # arrivals overlap the requests already running
         s.drain()
         got = [s.poll(i) for i in ids]
+        spans = [s.span(i) for i in ids]
     finally:
         s.close()
     for k, (g, a) in enumerate(zip(got, alone)):
@@ -78,6 +79,18 @@ def test_server_results_alone_and_in_the_mix(gpu):
         r, lat = g
         assert lat > 0
         assert (r.count, r.checksum, r.hist) == (a.count, a.checksum, a.hist), k
+    # the mix really shared the device: sweep the requests' device-clock spans
+    assert max_overlap(spans) >= 2, spans
+
+
+def max_overlap(spans):
+    """Largest number of [start, end) intervals that contain one instant."""
+    ev = sorted([(a, 1) for a, _ in spans] + [(b, -1) for _, b in spans], key=lambda t: (t[0], t[1]))
+    cur = best = 0
+    for _, d in ev:
+        cur += d
+        best = max(best, cur)
+    return best
 
 
 def test_server_rejects_unknown_request(gpu):

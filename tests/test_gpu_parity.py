@@ -227,3 +227,82 @@ def test_bin_roundtrip(gpu, oracle_mod, tmp_path):
     assert_same(r2, r1)
     oh = oracle_mod.Graph.load_bin(path)
     assert oh.mce(threads=THREADS).count == r1.count
+
+
+def hub_pair_graph(p_cols=3000, x_rows=20000, seed=8):
+    """Under the unchanged order, root (x_rows, x_rows + 1) is a hub pair with
+    p_cols candidates (sparse edges among them) and x_rows X rows, each with
+    one or two candidate neighbours, so no X row is dropped: an ego network of
+    (p_cols + x_rows) rows x ceil(p_cols / 64) words, far beyond the default
+    4 MB per-warp slab."""
+    rng = np.random.default_rng(seed)
+    X = np.arange(x_rows, dtype=np.int64)
+    v0, v1 = x_rows, x_rows + 1
+    P = np.arange(x_rows + 2, x_rows + 2 + p_cols, dtype=np.int64)
+    parts = [np.array([[v0, v1]])]
+    for hub in (v0, v1):
+        parts.append(np.stack([np.full(x_rows, hub), X], 1))
+        parts.append(np.stack([np.full(p_cols, hub), P], 1))
+    a = rng.integers(0, p_cols, size=3 * p_cols)
+    b = rng.integers(0, p_cols, size=3 * p_cols)
+    parts.append(np.stack([P[a], P[b]], 1))
+    for k in range(2):
+        keep = X if k == 0 else X[rng.random(x_rows) < 0.5]
+        parts.append(np.stack([keep, P[rng.integers(0, p_cols, size=len(keep))]], 1))
+    e = np.concatenate(parts).astype(np.uint32)
+    return e[:, 0].copy(), e[:, 1].copy()
+
+
+def test_hub_root_beyond_default_slab(gpu, oracle_mod):
+    """A root whose ego network exceeds the default slab is deferred to the
+    large-scratch pass and solved there (never skipped), in a full solve and
+    in per-root mode."""
+    u, v = hub_pair_graph()
+    _, o = oracle_result(oracle_mod, u, v)
+    with gpu.Graph.from_coo(u, v, opts(gpu, order=gpu.ORDER_UNCHANGED)) as g:
+        r = g.solve(opts(gpu))
+        assert r.heavy_roots >= 1
+        assert_same(r, o, "hub pair")
+        ro, ci, lab = g.export_csr()
+        og = oracle_mod.Graph.from_csr(ro.astype(np.uint64), ci, lab)
+        m = g.info()["num_edges"]
+        roots = np.unique(np.concatenate([np.arange(0, m, max(1, m // 300)), [og_root_id(og, 20000, 20001)]]))
+        roots = roots.astype(np.uint64)
+        ocnt, ochk = og.mce_roots(roots, threads=THREADS)
+        cnt, chk = g.solve_roots(roots, opts(gpu))
+    assert np.array_equal(cnt, ocnt) and np.array_equal(chk, ochk)
+
+
+def og_root_id(og, a, b):
+    """Root id of edge (a, b), a < b, in the CSR the oracle graph holds."""
+    off, adj, _ = og.export()
+    rid = 0
+    for x in range(a):
+        row = adj[off[x]:off[x + 1]]
+        rid += int((row > x).sum())
+    row = adj[off[a]:off[a + 1]]
+    return rid + int(((row > a) & (row < b)).sum())
+
+
+@pytest.mark.parametrize("heavy_warps", [3, 0])
+def test_deferred_roots_with_small_slabs(gpu, oracle_mod, heavy_warps):
+    """A 16 KiB slab cap defers every root with a wide ego network; the second
+    pass runs with 3 warps (a block smaller than the normal 8-warp block, one
+    slab per launched warp) or as many as memory allows.  Totals, histogram
+    and per-root values must match the oracle."""
+    u, v = gpu.gen_planted(600, 8, 60, 90, 11)
+    u2, v2 = gpu.gen_gnp(600, 20, 12)
+    u, v = np.concatenate([u, u2]), np.concatenate([v, v2])
+    _, o = oracle_result(oracle_mod, u, v)
+    small = dict(slab_kib=16, heavy_warps=heavy_warps)
+    with gpu.Graph.from_coo(u, v, opts(gpu)) as g:
+        r = g.solve(opts(gpu, **small))
+        assert r.heavy_roots > 0
+        assert_same(r, o, "small slabs")
+        assert_same(g.solve(opts(gpu, flags=gpu.FLAG_NO_SHARING, **small)), o, "small slabs, no sharing")
+        ro, ci, lab = g.export_csr()
+        og = oracle_mod.Graph.from_csr(ro.astype(np.uint64), ci, lab)
+        roots = np.arange(g.info()["num_edges"], dtype=np.uint64)
+        ocnt, ochk = og.mce_roots(roots, threads=THREADS)
+        cnt, chk = g.solve_roots(roots, opts(gpu, **small))
+    assert np.array_equal(cnt, ocnt) and np.array_equal(chk, ochk)
