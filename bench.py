@@ -339,10 +339,17 @@ def run_ours(args):
     def reduce(x, op):
         return reduce_over_ranks(x, op, world, dev)
 
-    stream = torch.cuda.current_stream(dev)
-    o = mce.options(device=local, stream=C.c_void_p(stream.cuda_stream))
     full = args.workload in FULL_WORKLOADS
     u, v = make_graph_pairs(args.workload)
+    ref_gpu = None
+    if args.ref_gpu and full and rank == 0:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+
+        expect = oracle.Graph.from_pairs(u, v).sort_degeneracy().mce(threads=os.cpu_count() or 1).count
+        ref_gpu = {"oracle_count": expect, "runs": reference_gpu_runs(u, v, expect)}
+    stream = torch.cuda.current_stream(dev)
+    o = mce.options(device=local, stream=C.c_void_p(stream.cuda_stream))
     g = mce.Graph.from_coo(u, v, o)
     info = g.info()
     roots = rank_roots(info["num_edges"], rank, world, full, args.sample)
@@ -493,6 +500,12 @@ def run_ours(args):
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if ref_gpu is not None:
+            line["reference_gpu"] = ref_gpu
+        if world == 1 and args.workload == "rmat20-sample" and not args.no_modes:
+            # the many-instance and serving modes, measured after the headline
+            line["batch"] = batch_measure(args)
+            line["serve"] = serve_measure(args)
         emit(line)
     g.close()
     if world > 1:
@@ -502,11 +515,59 @@ def run_ours(args):
     return 0
 
 
-def run_batch(args):
-    """Many-instance mode: the 10,000 G(n,p) + planted-clique members (n
+REF_GPU = {"stock": os.path.join(ROOT, "oracle", "_ref", "rdmce_ref_gpu"),
+           "no task sharing": os.path.join(ROOT, "oracle", "_ref", "rdmce_ref_gpu_noshare")}
+
+
+def reference_gpu_runs(u, v, expect, repeats=2):
+    """The reference's own CUDA build (unmodified sources, sm_100a) on the same
+    COO text, through its CLI `-i <file> -o deg -d 0` (main.cc): its count and
+    its "MCE GPU Time" (CSR upload + device setup + kernel, mce_gpu.cu:14-22).
+    Run before this process touches the GPU.  Each build runs `repeats` times
+    so a count that changes between runs shows."""
+    import numpy as np
+
+    runs = []
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "graph.txt")
+        with open(path, "w") as f:
+            for i in range(0, len(u), 1 << 20):
+                blk = np.stack([u[i:i + (1 << 20)], v[i:i + (1 << 20)]], axis=1)
+                f.write("\n".join(f"{a} {b}" for a, b in blk.tolist()))
+                f.write("\n")
+        for name, exe in REF_GPU.items():
+            if not os.path.exists(exe):
+                continue
+            for rep in range(repeats if name == "stock" else 1):
+                try:
+                    out = subprocess.run([exe, "-i", path, "-o", "deg", "-d", "0"], capture_output=True, text=True,
+                                         timeout=900)
+                except subprocess.TimeoutExpired:
+                    runs.append({"build": name, "run": rep, "error": "timed out after 900 s"})
+                    break
+                cnt = sec = None
+                for line in out.stdout.splitlines():
+                    if line.startswith("MC numbers:"):
+                        cnt = int(line.split(":")[1])
+                    if line.startswith("MCE GPU Time:"):
+                        sec = float(line.split(":")[1].strip().rstrip("s"))
+                rec = {"build": name, "run": rep, "count": cnt, "seconds": sec, "exit": out.returncode}
+                if cnt is not None and sec:
+                    rec["cliques_per_s"] = cnt / sec
+                    rec["count_matches_oracle"] = cnt == expect
+                runs.append(rec)
+    return runs
+
+
+BATCH_FIXTURE = os.path.join(ROOT, "tests", "golden", "samples", "batch_members.npz")
+SERVE_FIXTURE = os.path.join(ROOT, "tests", "golden", "samples", "serve_requests.json")
+
+
+def batch_measure(args):
+    """Many-instance mode (config: 10,000 G(n,p) + planted-clique members, n
     log-uniform in [64, 4096], degree uniform in [8, 64], seed 1000 + index)
-    enumerated in one captured persistent launch per step, against one plain
-    solve per graph on resident graphs."""
+    in one captured persistent launch per step, against one plain solve per
+    resident graph.  Every member is checked against the oracle fixture."""
     import numpy as np
     import torch
 
@@ -519,7 +580,7 @@ def run_batch(args):
     edges = sum(len(u) for u, _ in graphs)
     b = mce.Batch(graphs, o)
     for _ in range(args.warmup):
-        res, _, _ = b.solve(o)
+        res, hist, _ = b.solve(o)
     ref = [(r["count"], r["checksum"]) for r in res]
     times = []
     for _ in range(args.steps):
@@ -528,6 +589,15 @@ def run_batch(args):
             raise RuntimeError("batched results changed between steps")
         times.append(ms)
     b.close()
+    parity = "self-consistent across steps (no fixture)"
+    if os.path.exists(BATCH_FIXTURE):
+        fx = np.load(BATCH_FIXTURE)
+        if len(fx["count"]) == n:
+            got = np.array([[r["count"], r["checksum"], r["max_size"]] for r in res], np.uint64)
+            want = np.stack([fx["count"], fx["checksum"], fx["max_size"].astype(np.uint64)], 1)
+            if not (np.array_equal(got, want) and np.array_equal(np.asarray(hist, np.uint64), fx["hist"])):
+                raise RuntimeError("batched results differ from the oracle fixture")
+            parity = f"oracle-fixture ({n} members: count, checksum, largest clique, histogram)"
     value = n / (sum(times) / len(times) / 1000.0)
     # plain: one solve (one enumeration launch) per resident graph
     p = min(n, args.plain_graphs)
@@ -544,43 +614,61 @@ def run_batch(args):
     for h in handles:
         h.close()
     plain = p / plain_s
-    emit({"metric": "graphs/s (many-instance batch, one captured launch)", "value": value, "unit": "graphs/s",
-          "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sum(times) / len(times),
-          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-          "config": {"workload": f"{n} G(n,p) graphs, n log-uniform in [64, 4096], mean degree uniform in [8, 64], "
-                                 f"0-3 planted cliques of size 8-32, seed 1000 + index", "graphs": n,
-                     "pairs": int(edges), "cliques_per_step": int(sum(c for c, _ in ref))},
-          "plain_per_graph": {"value": plain, "unit": "graphs/s", "graphs_timed": p,
-                              "how": "mce_solve on each resident graph in turn, host wall clock"},
-          "batched_over_plain": value / plain})
-    return 0
+    return {"metric": "graphs/s (many-instance batch, one captured launch)", "value": value, "unit": "graphs/s",
+            "ms_per_step": sum(times) / len(times), "steps": args.steps,
+            "config": {"workload": f"{n} G(n,p) graphs, n log-uniform in [64, 4096], mean degree uniform in [8, 64], "
+                                   f"0-3 planted cliques of size 8-32, seed 1000 + index", "graphs": n,
+                       "pairs": int(edges), "cliques_per_step": int(sum(c for c, _ in ref))},
+            "parity": parity,
+            "plain_per_graph": {"value": plain, "unit": "graphs/s", "graphs_timed": p,
+                                "how": "mce_solve on each resident graph in turn, host wall clock"},
+            "batched_over_plain": value / plain,
+            "how": "CUDA events around the captured launch (graph replay) per step"}
 
 
-def run_serve(args):
-    """Request loop: Poisson arrivals (seed 5) of R-MAT requests, scale uniform
-    in [10, 13], edge factor uniform in [8, 32]; p50/p99 latency and cliques/s
-    against the same requests solved one after another."""
+def serve_requests(nreq):
+    """Request k: R-MAT with (scale, edge factor) drawn in order from
+    default_rng(5) -- scale uniform in [10, 13], edge factor uniform in [8, 32]
+    -- and graph seed 5000 + k; the same stream then draws the arrival gaps."""
+    import numpy as np
+
+    rng = np.random.default_rng(5)
+    return rng, [(int(rng.integers(10, 14)), int(rng.integers(8, 33)), 5000 + k) for k in range(nreq)]
+
+
+def serve_measure(args):
+    """Request loop: Poisson arrivals (seed 5) of R-MAT requests; p50/p99
+    latency and cliques/s per arrival rate, against the same requests solved
+    one after another.  Every served result is checked against the oracle
+    fixture (count, checksum, largest clique)."""
     import numpy as np
     import torch
 
     import rdmce_b200 as mce
 
     torch.cuda.set_device(0)
-    rng = np.random.default_rng(5)
-    nreq = args.serve_requests
-    reqs = [mce.gen_rmat(int(rng.integers(10, 14)), int(rng.integers(8, 33)), 5000 + k) for k in range(nreq)]
+    rng, spec = serve_requests(args.serve_requests)
+    reqs = [mce.gen_rmat(sc, ef, sd) for sc, ef, sd in spec]
+    want = None
+    if os.path.exists(SERVE_FIXTURE):
+        with open(SERVE_FIXTURE) as f:
+            fxr = json.load(f)["requests"]
+        if [(q["scale"], q["edge_factor"], q["seed"]) for q in fxr] == spec:
+            want = [(q["count"], q["checksum"], q["max_size"]) for q in fxr]
     o = mce.options(device=0)
     for u, v in reqs[:8]:
         mce.solve_coo(u, v, o)  # warm-up
     t0 = time.perf_counter()
     serial = [mce.solve_coo(u, v, o) for u, v in reqs]
     serial_s = time.perf_counter() - t0
+    if want is not None and [(r.count, f"{r.checksum:016x}", r.max_size) for r in serial] != want:
+        raise RuntimeError("serial solves differ from the oracle fixture")
     total = sum(r.count for r in serial)
     lines = []
     for rate in args.serve_rates:
-        gaps = rng.exponential(1.0 / rate, size=nreq)
+        gaps = rng.exponential(1.0 / rate, size=len(reqs))
         s = mce.Server(device=0)
-        ids, t_sub = [], []
+        ids = []
         start = time.perf_counter()
         due = start
         for (u, v), gap in zip(reqs, gaps):
@@ -591,22 +679,45 @@ def run_serve(args):
             ids.append(s.submit(u, v))
         s.drain()
         span = time.perf_counter() - start
-        lat = []
+        lat, spans = [], []
         for k, rid in enumerate(ids):
             r, ms = s.poll(rid)
             if (r.count, r.checksum) != (serial[k].count, serial[k].checksum):
                 raise RuntimeError(f"request {k}: served result differs from the solve alone")
             lat.append(ms)
+            spans.append(s.span(rid))
         s.close()
+        ev = sorted([(a, 1) for a, _ in spans] + [(b, -1) for _, b in spans])
+        cur = peak = 0
+        for _, d in ev:
+            cur += d
+            peak = max(peak, cur)
         lines.append({"rate_per_s": rate, "p50_ms": float(np.percentile(lat, 50)),
-                      "p99_ms": float(np.percentile(lat, 99)), "cliques_per_s": total / span,
-                      "span_s": span})
-    emit({"metric": "served maximal cliques/s and p50/p99 latency", "value": lines[-1]["cliques_per_s"],
-          "unit": "cliques/s", "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-          "dtype": "u64", "data": "synthetic",
-          "config": {"workload": f"{nreq} R-MAT requests, scale uniform in [10, 13], edge factor uniform in "
-                                 f"[8, 32], Poisson arrivals seed 5", "cliques": int(total)},
-          "rates": lines, "serial_plain": {"cliques_per_s": total / serial_s, "seconds": serial_s}})
+                      "p99_ms": float(np.percentile(lat, 99)), "cliques_per_s": total / span, "span_s": span,
+                      "peak_requests_on_device": peak})
+    return {"metric": "served maximal cliques/s and p50/p99 latency", "value": lines[-1]["cliques_per_s"],
+            "unit": "cliques/s",
+            "config": {"workload": f"{len(reqs)} R-MAT requests, scale uniform in [10, 13], edge factor uniform in "
+                                   f"[8, 32], Poisson arrivals seed 5, request k seeded 5000 + k",
+                       "cliques": int(total)},
+            "parity": "oracle-fixture (every request: count, checksum, largest clique)" if want is not None else
+                      "served == solved alone",
+            "rates": lines, "serial_plain": {"cliques_per_s": total / serial_s, "seconds": serial_s},
+            "how": "host wall clock from first arrival to the last completion; peak_requests_on_device from the "
+                   "requests' device-clock spans (mce_server_request_span)"}
+
+
+def run_batch(args):
+    line = batch_measure(args)
+    emit({**line, "n_gpus": 1, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+          "vs_baseline": None, "dtype": "u64", "data": "synthetic"})
+    return 0
+
+
+def run_serve(args):
+    line = serve_measure(args)
+    emit({**line, "n_gpus": 1, "steps": len(args.serve_rates), "warmup": 8, "higher_is_better": True,
+          "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic"})
     return 0
 
 
@@ -638,6 +749,10 @@ def main():
     ap.add_argument("--plain-graphs", type=int, default=1000, help="graphs timed with one plain solve each")
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[10.0, 100.0, 2000.0])
+    ap.add_argument("--ref-gpu", action="store_true",
+                    help="full workloads: also run the reference's own CUDA builds on the same graph")
+    ap.add_argument("--no-modes", action="store_true",
+                    help="headline only: skip the batch and serve objects of the default line")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")

@@ -26,7 +26,9 @@ import networkx as nx
 HERE = os.path.dirname(os.path.abspath(__file__))
 M64 = (1 << 64) - 1
 G = 0x9E3779B97F4A7C15
-REF_ZACHARY = "/root/reference/RDMCE/data/zachary.txt"
+# the reference's own data/zachary.txt, found through RDMCE_REFERENCE (the
+# RDMCE/ directory of the reference tree); skipped when that is not set
+REF_ZACHARY = os.path.join(os.environ.get("RDMCE_REFERENCE", ""), "data", "zachary.txt")
 
 
 def mix64(x: int) -> int:

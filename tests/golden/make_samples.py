@@ -101,39 +101,71 @@ def make_rmat20(threads):
     return rec
 
 
+def root_ids_of_edges(g, a, b):
+    """Root ids of edges (a, b) with a < b in g's CSR: a's first root plus
+    b's rank among a's later neighbours."""
+    off, adj, _ = g.export()
+    n = g.n
+    row = np.repeat(np.arange(n, dtype=np.uint32), np.diff(off).astype(np.int64))
+    upper = adj > row
+    first = np.zeros(n + 1, np.uint64)
+    np.cumsum(np.bincount(row[upper], minlength=n).astype(np.uint64), out=first[1:])
+    out = np.empty(len(a), np.uint64)
+    for k, (x, y) in enumerate(zip(a, b)):
+        nb = adj[off[x]:off[x + 1]]
+        out[k] = first[x] + np.searchsorted(nb[nb > x], y)
+    return out
+
+
 def make_rmat24(threads, per_stratum, root_budget_s):
     """Roots stratified by candidate-set size p (the ego network's column
-    count), each kept only if the oracle solves it within root_budget_s on one
-    thread, so the fixture stays cheap to regenerate.  Hub-hub roots with
-    astronomically many cliques are thereby left to the internal-consistency
-    checks; every p stratum up to the degeneracy is still represented."""
+    count), plus roots inside planted cliques; each kept only if the oracle
+    solves it within root_budget_s on one thread, so the fixture stays cheap to
+    regenerate.  Roots of the dense core with astronomically many cliques are
+    thereby left to the internal-consistency checks."""
+    from concurrent.futures import ThreadPoolExecutor
+
     import oracle
     import rdmce_b200 as mce
 
-    u, v = rmat24_pairs(mce)
+    c = RMAT24
+    u, v = mce.gen_rmat(c["scale"], c["edge_factor"], c["seed"])
+    pu, pv = mce.gen_planted(1 << c["scale"], c["planted"], c["planted_lo"], c["planted_hi"], c["planted_seed"])
     t = time.time()
-    g = ordered_oracle_graph(oracle, u, v)
+    g = ordered_oracle_graph(oracle, np.concatenate([u, pu]), np.concatenate([v, pv]))
+    del u, v
     print(f"rmat24: ordered graph n={g.n} m={g.m} k={g.degeneracy} in {time.time() - t:.0f} s", flush=True)
     rec = {"graph": dict(RMAT24, generator="rdmce_b200.gen_rmat + rdmce_b200.gen_planted"), **graph_record(g)}
     rng = np.random.default_rng(777)
-    strata = [(0, 1), (1, 8), (8, 32), (32, 64), (64, 128), (128, 256), (256, 512), (512, 1024), (1024, 1 << 20)]
-    chosen = []
-    probe = np.sort(rng.choice(g.m, size=min(g.m, 400000), replace=False)).astype(np.uint64)
+    probe = np.sort(rng.choice(g.m, size=min(g.m, 20000), replace=False)).astype(np.uint64)
     sizes = g.root_sizes_list(probe)
-    for lo, hi in strata:
-        pool = probe[(sizes >= lo) & (sizes < hi)]
-        rng.shuffle(pool)
-        kept = 0
-        for r in pool[: 20 * per_stratum]:
-            res, started, el = g.mce_roots_timed(np.array([r], np.uint64), 1, root_budget_s)
-            if el < root_budget_s * 0.95:
-                chosen.append(int(r))
-                kept += 1
-                if kept == per_stratum:
-                    break
-        print(f"rmat24: p in [{lo},{hi}): {kept} roots from {len(pool)} candidates", flush=True)
-    roots = np.array(sorted(chosen), np.uint64)
-    rec["sample"] = f"stratified by p, {per_stratum} per stratum, each solvable by the oracle in {root_budget_s} s"
+    # planted-clique edges, as root ids of the ordered graph
+    _, _, lab = g.export()
+    order = np.argsort(lab)
+    idx = rng.choice(len(pu), size=400, replace=False)
+    ia = order[np.searchsorted(lab[order], pu[idx])]
+    ib = order[np.searchsorted(lab[order], pv[idx])]
+    planted = root_ids_of_edges(g, np.minimum(ia, ib), np.maximum(ia, ib))
+    strata = [(0, 1), (1, 8), (8, 32), (32, 64), (64, 128), (128, 256), (256, 512), (512, 1024), (1024, 1 << 20)]
+    pools = [(f"p in [{lo},{hi})", probe[(sizes >= lo) & (sizes < hi)], per_stratum) for lo, hi in strata]
+    pools.append(("inside a planted clique", np.unique(planted), 2 * per_stratum))
+
+    def solvable(r):
+        _, _, el = g.mce_roots_timed(np.array([r], np.uint64), 1, root_budget_s)
+        return el < root_budget_s * 0.95
+
+    chosen = []
+    with ThreadPoolExecutor(threads) as ex:
+        for name, pool, want in pools:
+            pool = pool.copy()
+            rng.shuffle(pool)
+            cand = [int(r) for r in pool[: 4 * want]]
+            ok = [r for r, good in zip(cand, ex.map(solvable, cand)) if good][:want]
+            chosen += ok
+            print(f"rmat24: {name}: {len(ok)} roots kept of {len(cand)} tried ({len(pool)} in the pool)", flush=True)
+    roots = np.array(sorted(set(chosen)), np.uint64)
+    rec["sample"] = (f"{per_stratum} roots per p stratum of a 20,000-root probe and {2 * per_stratum} inside planted "
+                     f"cliques, each solvable by the oracle in {root_budget_s} s on one thread")
     rec["strata"] = strata
     rec["p"] = [int(x) for x in g.root_sizes_list(roots)]
     rec.update(solve_record(g, roots, threads))
@@ -197,7 +229,7 @@ def main():
     ap.add_argument("what", choices=["rmat20", "rmat24", "batch", "serve"])
     ap.add_argument("--threads", type=int, default=os.cpu_count() or 1)
     ap.add_argument("--per-stratum", type=int, default=3)
-    ap.add_argument("--root-budget", type=float, default=20.0)
+    ap.add_argument("--root-budget", type=float, default=10.0)
     ap.add_argument("--batch-count", type=int, default=10000)
     a = ap.parse_args()
     os.makedirs(OUT, exist_ok=True)

@@ -110,3 +110,39 @@ def test_engine_order_equals_oracle_restatement(gpu, oracle_mod, name):
     assert np.array_equal(ro.astype(np.uint64), off)
     assert np.array_equal(ci, adj)
     assert np.array_equal(lab, olab)
+
+
+def test_batch_all_members_match_fixture(gpu):
+    """All 10,000 many-instance members (G(n,p) + planted cliques, seed
+    1000 + index) in one captured launch, each against the oracle: count,
+    checksum, largest clique and histogram (sizes >= 63 in the last bin)."""
+    path = os.path.join(SAMPLES, "batch_members.npz")
+    if not os.path.exists(path):
+        pytest.skip("batch_members.npz not generated")
+    fx = np.load(path)
+    n = len(fx["count"])
+    graphs = [gpu.gen_batch_member(i)[:2] for i in range(n)]
+    b = gpu.Batch(graphs, opts(gpu))
+    try:
+        res, hist, _ = b.solve(opts(gpu), hist_len=fx["hist"].shape[1])
+    finally:
+        b.close()
+    assert np.array_equal(np.array([r["count"] for r in res], np.uint64), fx["count"])
+    assert np.array_equal(np.array([r["checksum"] for r in res], np.uint64), fx["checksum"])
+    assert np.array_equal(np.array([r["max_size"] for r in res], np.uint32), fx["max_size"])
+    assert np.array_equal(np.asarray(hist, np.uint64), fx["hist"])
+
+
+def test_served_requests_match_fixture(gpu):
+    """The serving loop's 200 requests (R-MAT, scale 10-13, edge factor 8-32),
+    submitted back to back so they share the device, each against the oracle."""
+    fx = load("serve_requests.json")["requests"]
+    s = gpu.Server(device=0)
+    try:
+        ids = [s.submit(*gpu.gen_rmat(q["scale"], q["edge_factor"], q["seed"])) for q in fx]
+        s.drain()
+        got = [s.poll(i)[0] for i in ids]
+    finally:
+        s.close()
+    for q, r in zip(fx, got):
+        assert (r.count, f"{r.checksum:016x}", r.max_size) == (q["count"], q["checksum"], q["max_size"]), q
