@@ -55,6 +55,7 @@ METRIC = "maximal cliques/s"
 UNIT = "cliques/s"
 REF_CPU = os.path.join(ROOT, "oracle", "_ref", "ref_cpu")
 FIXTURE = os.path.join(ROOT, "tests", "golden", "samples", "rmat20_sample.json")
+FIXTURE24 = os.path.join(ROOT, "tests", "golden", "samples", "rmat24_sample.json")
 # roots below this many cliques finish in well under a second on one core:
 # the reference arm solves them to completion as its parity check
 LIGHT_ROOT = 10_000_000
@@ -80,6 +81,9 @@ def workload_name(sample, workload="rmat20-sample"):
     if workload in FULL_WORKLOADS:
         sc, ef, sd = FULL_WORKLOADS[workload]
         return f"R-MAT scale {sc}, edge factor {ef}, a/b/c/d=0.57/0.19/0.19/0.05, seed {sd}; full enumeration"
+    if workload == "rmat24-sample":
+        return ("R-MAT scale 24, edge factor 32, a/b/c/d=0.57/0.19/0.19/0.05, seed 3, plus 256 planted cliques of "
+                f"40-200 vertices; all maximal cliques under {sample} seeded random edge roots per step")
     return (f"R-MAT scale {SCALE}, edge factor {EDGE_FACTOR}, a/b/c/d=0.57/0.19/0.19/0.05, seed {GRAPH_SEED}; "
             f"all maximal cliques under {sample} seeded random edge roots per rank per step")
 
@@ -142,8 +146,16 @@ def dist_env():
 
 
 def make_graph_pairs(workload="rmat20-sample"):
+    import numpy as np
+
     import rdmce_b200 as mce
 
+    if workload == "rmat24-sample":
+        # R-MAT scale 24, edge factor 32, seed 3, plus 256 planted cliques of
+        # 40-200 vertices on uniform random vertex sets (planted seed 3)
+        u, v = mce.gen_rmat(24, 32, 3)
+        pu, pv = mce.gen_planted(1 << 24, 256, 40, 200, 3)
+        return np.concatenate([u, pu]), np.concatenate([v, pv])
     if workload == "chunglu":
         return mce.gen_chung_lu(10000, 16, 2.5, 1)
     if workload in FULL_WORKLOADS:
@@ -372,12 +384,28 @@ def run_ours(args):
         ref = (r.count, r.checksum)
     # parity: the headline sample must reproduce the CPU oracle's fixture
     fx = None
+    parity = "self-consistent across steps (no fixture)"
     if args.workload == "rmat20-sample" and rank == 0 and os.path.exists(FIXTURE):
         fx = load_fixture()
         if len(fx["roots"]) != len(roots) or [int(x) for x in roots] != fx["roots"]:
             fx = None
         else:
             check_fixture(g, r, fx)
+            parity = "oracle-fixture"
+    if args.workload == "rmat24-sample" and rank == 0 and os.path.exists(FIXTURE24):
+        # the timed roots are too heavy for the oracle: the fixture's
+        # stratified roots are checked on the same resident graph (untimed),
+        # and the timed sample must agree with itself with and without sharing
+        with open(FIXTURE24) as f:
+            fx24 = json.load(f)
+        r24 = g.solve_root_list(np.array(fx24["roots"], np.uint64), o)
+        check_fixture(g, r24, fx24)
+        ns = g.solve_root_list(roots, mce.options(device=local, stream=C.c_void_p(stream.cuda_stream),
+                                                  flags=mce.FLAG_NO_SHARING))
+        if (ns.count, ns.checksum) != ref:
+            raise RuntimeError("timed sample differs without task sharing")
+        parity = (f"oracle-fixture on {len(fx24['roots'])} stratified roots of the same graph; timed sample "
+                  f"identical with and without task sharing")
     clocks = Clocks(local)
     barrier()
     torch.cuda.synchronize()
@@ -476,7 +504,7 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": 1000.0 * t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": config,
-            "parity": "oracle-fixture" if fx is not None else "self-consistent across steps (no fixture)",
+            "parity": parity,
             "roofline": {"bound": "int", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gword-ops/s",
                          "frac": achieved / peak if peak else None, "traffic": None,
                          "note": "bitmap row word-ops of one step (ANDN+POPC per active row per node, row "
@@ -739,9 +767,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--sample", type=int, default=DEFAULT_SAMPLE, help="edge roots per rank per step")
-    ap.add_argument("--workload", choices=["rmat20-sample"] + sorted(FULL_WORKLOADS), default="rmat20-sample",
-                    help="the headline root sample of R-MAT scale 20, or a smaller graph enumerated in full")
+    ap.add_argument("--sample", type=int, default=None,
+                    help=f"edge roots per rank per step (default {DEFAULT_SAMPLE}; 16 for rmat24-sample)")
+    ap.add_argument("--workload", choices=["rmat20-sample", "rmat24-sample"] + sorted(FULL_WORKLOADS),
+                    default="rmat20-sample",
+                    help="the headline root sample of R-MAT scale 20, the R-MAT 24 + planted-clique sample, or a "
+                         "smaller graph enumerated in full")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU oracle time bound (0 = skip)")
     ap.add_argument("--mode", choices=["solve", "batch", "serve"], default="solve",
                     help="solve: the headline; batch: many-instance graphs/s; serve: the request loop")
@@ -754,6 +785,8 @@ def main():
     ap.add_argument("--no-modes", action="store_true",
                     help="headline only: skip the batch and serve objects of the default line")
     args = ap.parse_args()
+    if args.sample is None:
+        args.sample = 16 if args.workload == "rmat24-sample" else DEFAULT_SAMPLE
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
     if args.impl == "reference":

@@ -99,6 +99,9 @@ typedef struct mce_result {
   uint64_t heavy_roots;       /* roots that went through the large-scratch pass */
   uint64_t nodes;             /* search-tree nodes visited (with MCE_FLAG_STATS, else 0) */
   uint64_t word_ops;          /* bitmap row word operations (AND/ANDN/POPC; with MCE_FLAG_STATS) */
+  uint64_t build_bytes;       /* algorithmic bytes of the roots' ego-network builds (with MCE_FLAG_STATS):
+                                 per root 4 (d(v0) + d(v1)) + sum over members u of P and X of
+                                 (4 d(u) + 8 W), W = ceil(|P| / 64) */
   uint64_t launches;          /* enumeration kernel launches */
   uint64_t warp_cycles[6];    /* warp clock cycles by phase: root build, register tiers,
                                  general tier, exposing tasks, idle, queue */
@@ -178,7 +181,9 @@ mce_status mce_graph_from_csr(uint64_t n, const uint32_t *rowoffset, const uint3
 
 /* COO text (Graph::LoadFromFile, src/graph.cc:64-152) or the reference .bin
  * container (Graph::LoadFromBin, src/graph.cc:178-213), chosen by the .bin
- * suffix exactly as main.cc:181-191 does. */
+ * suffix exactly as main.cc:181-191 does.  Text is parsed on the GPU (the
+ * file streamed to device memory, records found and converted there) and the
+ * pairs go straight to the device graph build. */
 mce_status mce_graph_load_file(const char *path, const mce_options *opt, mce_graph **out);
 
 /* Write the reference .bin container (Graph::StoreIntoBin, src/graph.cc:154-176). */
@@ -273,6 +278,10 @@ mce_status mce_gen_batch_member(uint32_t index, uint64_t base_seed, uint32_t *u,
 /* COO text parse with the reference's istream semantics (src/graph.cc:82-104).
  * Buffers are malloc'ed; release them with mce_free_host. */
 mce_status mce_parse_text(const char *path, uint32_t **u, uint32_t **v, uint64_t *n_pairs);
+/* The same parse on the GPU of `device` (the one mce_graph_load_file uses for
+ * text), results copied back into malloc'ed host buffers (mce_free_host).
+ * Replaces the text loop of Graph::LoadFromFile (src/graph.cc:82-104). */
+mce_status mce_parse_text_gpu(const char *path, int device, uint32_t **u, uint32_t **v, uint64_t *n_pairs);
 void mce_free_host(void *p);
 
 #ifdef __cplusplus

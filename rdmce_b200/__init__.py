@@ -75,6 +75,7 @@ class _Result(C.Structure):
         ("heavy_roots", C.c_uint64),
         ("nodes", C.c_uint64),
         ("word_ops", C.c_uint64),
+        ("build_bytes", C.c_uint64),
         ("launches", C.c_uint64),
         ("warp_cycles", C.c_uint64 * 6),
         ("max_item_cycles", C.c_uint64 * 2),
@@ -132,13 +133,14 @@ class Result:
     # warp clock cycles: root build, register tiers, general tier, exposing tasks, idle, queue
     warp_cycles: list = field(default_factory=list)
     max_item_cycles: list = field(default_factory=list)
+    build_bytes: int = 0
 
     @classmethod
     def _from(cls, r: _Result) -> "Result":
         hist = {s: int(r.hist[s]) for s in range(HIST_LEN) if r.hist[s]}
         return cls(r.count, r.checksum, hist, r.max_size, r.degeneracy, r.max_degree, r.num_vertices,
                    r.num_edges, r.roots, r.shared_tasks, r.heavy_roots, list(r.phase_ms), r.nodes, r.word_ops,
-                   r.launches, list(r.warp_cycles), list(r.max_item_cycles))
+                   r.launches, list(r.warp_cycles), list(r.max_item_cycles), r.build_bytes)
 
 
 _lib = None
@@ -180,6 +182,7 @@ _SIGS = {
     "mce_gen_planted": (_I, [_U32, _U32, _U32, _U32, _U64, _P, _P, _U64, C.POINTER(_U64)]),
     "mce_gen_batch_member": (_I, [_U32, _U64, _P, _P, _U64, C.POINTER(_U64), C.POINTER(_U32)]),
     "mce_parse_text": (_I, [C.c_char_p, C.POINTER(_P), C.POINTER(_P), C.POINTER(_U64)]),
+    "mce_parse_text_gpu": (_I, [C.c_char_p, _I, C.POINTER(_P), C.POINTER(_P), C.POINTER(_U64)]),
     "mce_free_host": (None, [_P]),
 }
 
@@ -284,10 +287,16 @@ def gen_batch_member(index, base_seed=1000):
     return u[:k], v[:k], nv.value
 
 
-def parse_text(path: str):
+def parse_text(path: str, device: int | None = None):
+    """COO text with the reference parser's semantics: on the host, or on the
+    GPU `device` (the path mce_graph_load_file takes for text)."""
     L = lib()
     pu, pv, n = C.c_void_p(), C.c_void_p(), C.c_uint64()
-    _check(L.mce_parse_text(path.encode(), C.byref(pu), C.byref(pv), C.byref(n)), "mce_parse_text")
+    if device is None:
+        _check(L.mce_parse_text(path.encode(), C.byref(pu), C.byref(pv), C.byref(n)), "mce_parse_text")
+    else:
+        _check(L.mce_parse_text_gpu(path.encode(), device, C.byref(pu), C.byref(pv), C.byref(n)),
+               "mce_parse_text_gpu")
     k = n.value
     if k:
         u = np.ctypeslib.as_array(C.cast(pu, C.POINTER(C.c_uint32)), shape=(k,)).copy()

@@ -256,9 +256,59 @@ mce_status mce_graph_load_file(const char *path, const mce_options *opt, mce_gra
     *out = h;
     return MCE_OK;
   }
-  std::vector<uint32_t> u, v;
-  MCE_TRY(parse_coo_text(path, u, v));
-  return mce_graph_from_coo(u.data(), v.data(), u.size(), opt, out);
+  // COO text: parsed on the GPU straight into the device COO buffers
+  mce_options tmp;
+  const mce_options &o = opts_or_default(opt, tmp);
+  mce_graph *h = nullptr;
+  MCE_TRY(new_handle(o, &h));
+  Timer t;
+  uint32_t *ud = nullptr, *vd = nullptr;
+  uint64_t np = 0;
+  mce_status s = parse_text_device(path, h->stream, &ud, &vd, &np);
+  h->ms_h2d = t.ms();
+  if (s == MCE_OK) s = graph_from_device_pairs(ud, vd, np, o, h);
+  if (ud) cudaFreeAsync(ud, h->stream);
+  if (vd) cudaFreeAsync(vd, h->stream);
+  if (s != MCE_OK) {
+    cudaGetLastError();
+    destroy_handle(h);
+    return s;
+  }
+  *out = h;
+  return MCE_OK;
+}
+
+mce_status mce_parse_text_gpu(const char *path, int device, uint32_t **u, uint32_t **v, uint64_t *n_pairs) {
+  if (!path || !u || !v || !n_pairs) return MCE_ERR_INVALID_ARG;
+  *u = *v = nullptr;
+  *n_pairs = 0;
+  MCE_TRY(set_device(device));
+  cudaStream_t st = nullptr;
+  MCE_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  uint32_t *ud = nullptr, *vd = nullptr;
+  uint64_t np = 0;
+  mce_status s = parse_text_device(path, st, &ud, &vd, &np);
+  if (s == MCE_OK) {
+    *u = (uint32_t *)std::malloc(std::max<uint64_t>(np, 1) * 4);
+    *v = (uint32_t *)std::malloc(std::max<uint64_t>(np, 1) * 4);
+    if (!*u || !*v) s = MCE_ERR_OUT_OF_MEMORY;
+  }
+  if (s == MCE_OK && np &&
+      (cudaMemcpyAsync(*u, ud, np * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+       cudaMemcpyAsync(*v, vd, np * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess))
+    s = MCE_ERR_CUDA;
+  if (ud) cudaFreeAsync(ud, st);
+  if (vd) cudaFreeAsync(vd, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && s == MCE_OK) s = MCE_ERR_CUDA;
+  cudaStreamDestroy(st);
+  if (s != MCE_OK) {
+    std::free(*u);
+    std::free(*v);
+    *u = *v = nullptr;
+    return s;
+  }
+  *n_pairs = np;
+  return MCE_OK;
 }
 
 mce_status mce_graph_info_get(const mce_graph *g, mce_graph_info *info) {
@@ -349,6 +399,7 @@ static mce_status solve_impl(mce_graph *g, const mce_options &o, mce_result *out
   out->shared_tasks = stats.shared_tasks;
   out->nodes = stats.nodes;
   out->word_ops = stats.word_ops;
+  out->build_bytes = stats.build_bytes;
   out->launches = stats.launches;
   for (int i = 0; i < 6; i++) out->warp_cycles[i] = stats.cycles[i];
   for (int i = 0; i < 2; i++) out->max_item_cycles[i] = stats.max_item[i];

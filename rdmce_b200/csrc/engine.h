@@ -38,6 +38,11 @@ mce_status build_from_csr(uint64_t n, const uint32_t *off_d, const uint32_t *adj
 mce_status csr_to_edges(uint64_t n, const uint32_t *off, const uint32_t *adj, uint64_t m, uint32_t *deg,
                         uint32_t **eu, uint32_t **ev, cudaStream_t st);
 void free_graph(DeviceGraph *g);
+// COO text file -> pairs in device memory (ingest.cu), with the reference
+// parser's semantics; *u_out / *v_out are cudaMallocAsync'ed on st (free with
+// cudaFreeAsync)
+mce_status parse_text_device(const char *path, cudaStream_t st, uint32_t **u_out, uint32_t **v_out,
+                             uint64_t *n_out);
 
 struct EnumConfig {
   uint32_t warps_per_block = 0;
@@ -92,7 +97,7 @@ struct EnumStats {
   uint64_t roots = 0;
   uint64_t heavy_roots = 0;
   uint64_t shared_tasks = 0;
-  uint64_t nodes = 0, word_ops = 0;
+  uint64_t nodes = 0, word_ops = 0, build_bytes = 0;
   uint64_t cycles[6] = {0, 0, 0, 0, 0, 0};
   uint64_t max_item[2] = {0, 0};  // longest root, longest task (cycles)
   uint32_t error = 0;
@@ -143,6 +148,7 @@ struct EnumParams {
   unsigned long long *stat_tasks;
   unsigned long long *stat_nodes;
   unsigned long long *stat_wops;
+  unsigned long long *stat_bbytes;       // algorithmic ego-network build bytes (stats mode)
   unsigned long long *stat_cycles;       // per phase: build, register tiers, general tier, spawn, idle, queue
   unsigned long long *stat_max_item;     // [2]: longest root, longest task, in cycles
   unsigned int *active;                  // warps holding work

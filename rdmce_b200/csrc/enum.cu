@@ -125,7 +125,7 @@ struct WarpSmem {
   uint32_t share_period;
   uint32_t hcache[kHistCache];
   // result accumulators for the current slot
-  unsigned long long count, checksum, nodes, wops;
+  unsigned long long count, checksum, nodes, wops, bbytes;
   uint32_t max_size, slot, pending, pad;
   unsigned long long cyc[kCycPhases];  // clock64 cycles by phase
   // The tiers enclosing the running subproblem.  A nested tier exposes their
@@ -1740,16 +1740,27 @@ __device__ bool solve_root(const Ctx &c, uint64_t r) {
   const uint32_t x = nc ? lower_bound_u32(cand, nc, v1) : 0;
   const uint32_t p = nc - x;
   const uint64_t s1 = g.h1[v0] + g.h1[v1], s2 = g.h2[v0] + g.h2[v1];
+  const uint32_t W = (p + 63) / 64;
+  const Layout L = layout_for(nc, p, p + x, W);
+  if (p > 0 && L.need > c.slab_bytes) {
+    if (c.lane == 0) c.sm->cyc[kCycBuild] += now() - tb0;
+    return false;
+  }
+  if (c.P->stats) {
+    // algorithmic build bytes: both endpoint lists, then every member's
+    // adjacency list and its bitmap row
+    uint64_t du = 0;
+    if (p > 0)
+      for (uint32_t j = c.lane; j < nc; j += 32) du += g.off[cand[j] + 1] - g.off[cand[j]];
+    du = warp_sum_u64(du);
+    if (c.lane == 0)
+      c.sm->bbytes += 4ULL * ((g.off[v0 + 1] - g.off[v0]) + (g.off[v1 + 1] - g.off[v1])) +
+                      (p > 0 ? 4ULL * du + 8ULL * W * nc : 0);
+  }
   if (p == 0) {
     if (x == 0 && c.lane == 0) emit(c, 2, s1, s2);
     if (c.lane == 0) c.sm->cyc[kCycBuild] += now() - tb0;
     return true;
-  }
-  const uint32_t W = (p + 63) / 64;
-  const Layout L = layout_for(nc, p, p + x, W);
-  if (L.need > c.slab_bytes) {
-    if (c.lane == 0) c.sm->cyc[kCycBuild] += now() - tb0;
-    return false;
   }
   uint64_t *rows = (uint64_t *)(c.slab + L.rows_off);
   const uint32_t nrows = build_rows(g, cand, x, p, W, rows, c.sm->rowbuf);
@@ -1871,7 +1882,7 @@ __global__ void __launch_bounds__(256, 4) k_enumerate(const __grid_constant__ En
   c.sm = sm;
   for (uint32_t b = c.lane; b < kHistCache; b += 32) sm->hcache[b] = 0;
   if (c.lane == 0) {
-    sm->count = sm->checksum = sm->nodes = sm->wops = 0;
+    sm->count = sm->checksum = sm->nodes = sm->wops = sm->bbytes = 0;
     sm->max_size = sm->slot = sm->pending = 0;
     sm->nest = 0;
     sm->share_period = kShareMin;
@@ -2032,6 +2043,7 @@ __global__ void __launch_bounds__(256, 4) k_enumerate(const __grid_constant__ En
     if (P.stats) {
       atomicAdd(P.stat_nodes, sm->nodes);
       atomicAdd(P.stat_wops, sm->wops);
+      atomicAdd(P.stat_bbytes, sm->bbytes);
     }
     for (int i = 0; i < kCycPhases; i++) atomicAdd(P.stat_cycles + i, sm->cyc[i]);
   }
@@ -2045,7 +2057,7 @@ struct EnumCtl {
   alignas(128) unsigned long long ready_head;
   alignas(128) unsigned long long ready_tail;
   alignas(128) unsigned int active;
-  alignas(128) unsigned long long heavy_need, stat_roots, stat_tasks, stat_nodes, stat_wops;
+  alignas(128) unsigned long long heavy_need, stat_roots, stat_tasks, stat_nodes, stat_wops, stat_bbytes;
   unsigned long long stat_cycles[kCycPhases];
   unsigned long long stat_max_item[2];
   unsigned int heavy_n, error;
@@ -2137,6 +2149,7 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
   P.stat_tasks = &ctl->stat_tasks;
   P.stat_nodes = &ctl->stat_nodes;
   P.stat_wops = &ctl->stat_wops;
+  P.stat_bbytes = &ctl->stat_bbytes;
   P.stat_cycles = ctl->stat_cycles;
   P.stat_max_item = ctl->stat_max_item;
   P.active = &ctl->active;
@@ -2238,7 +2251,7 @@ mce_status enum_finish(const EnumPlan &plan, cudaStream_t st, EnumStats *stats) 
   const uint64_t heavy_roots = h.heavy_n;
   uint64_t launches = plan.nwork ? 1 : 0;
   uint64_t roots = h.stat_roots;
-  uint64_t tasks = h.stat_tasks, nodes = h.stat_nodes, wops = h.stat_wops;
+  uint64_t tasks = h.stat_tasks, nodes = h.stat_nodes, wops = h.stat_wops, bbytes = h.stat_bbytes;
   uint64_t cycles[kCycPhases];
   for (int i = 0; i < kCycPhases; i++) cycles[i] = h.stat_cycles[i];
   uint64_t max_item[2] = {h.stat_max_item[0], h.stat_max_item[1]};
@@ -2287,6 +2300,7 @@ mce_status enum_finish(const EnumPlan &plan, cudaStream_t st, EnumStats *stats) 
     tasks += h2.stat_tasks;
     nodes += h2.stat_nodes;
     wops += h2.stat_wops;
+    bbytes += h2.stat_bbytes;
     for (int i = 0; i < kCycPhases; i++) cycles[i] += h2.stat_cycles[i];
     for (int i = 0; i < 2; i++) max_item[i] = std::max<uint64_t>(max_item[i], h2.stat_max_item[i]);
     err = h2.error;
@@ -2297,6 +2311,7 @@ mce_status enum_finish(const EnumPlan &plan, cudaStream_t st, EnumStats *stats) 
     stats->shared_tasks = tasks;
     stats->nodes = nodes;
     stats->word_ops = wops;
+    stats->build_bytes = bbytes;
     for (int i = 0; i < kCycPhases; i++) stats->cycles[i] = cycles[i];
     for (int i = 0; i < 2; i++) stats->max_item[i] = max_item[i];
     stats->error = err;

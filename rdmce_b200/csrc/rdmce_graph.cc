@@ -39,13 +39,15 @@ void Graph::Require(mce_status s, const char *what) const {
 
 void Graph::LoadFromFile(const std::string &path) {
   name_ = ExtractName(path);
-  uint32_t *u = nullptr, *v = nullptr;
-  uint64_t n = 0;
-  Require(mce_parse_text(path.c_str(), &u, &v, &n), ("cannot read " + path).c_str());
-  u_.assign(u, u + n);
-  v_.assign(v, v + n);
-  mce_free_host(u);
-  mce_free_host(v);
+  // the text is parsed on the GPU when the device graph is built (Handle),
+  // with the order chosen by then; only its readability is checked here, so a
+  // missing file still fails at load time as the reference's does
+  FILE *f = std::fopen(path.c_str(), "rb");
+  if (!f) throw Error(MCE_ERR_IO, "cannot read " + path);
+  std::fclose(f);
+  text_path_ = path;
+  u_.clear();
+  v_.clear();
   mce_graph_free(g_);
   g_ = nullptr;
   rowoffset_.clear();
@@ -60,6 +62,7 @@ void Graph::LoadFromBin(const std::string &path) {
   mce_graph_free(g_);
   g_ = nullptr;
   Require(mce_graph_load_file(path.c_str(), &o, &g_), ("cannot load " + path).c_str());
+  text_path_.clear();
   u_.clear();
   v_.clear();
   rowoffset_.clear();
@@ -77,13 +80,16 @@ mce_graph *Graph::Handle() {
       case OrderType::DES: o.order = MCE_ORDER_DEGREE_DESC; break;
       case OrderType::DEG: o.order = MCE_ORDER_DEGENERACY; break;
     }
-    Require(mce_graph_from_coo(u_.data(), v_.data(), u_.size(), &o, &g_), "graph build");
+    if (!text_path_.empty())
+      Require(mce_graph_load_file(text_path_.c_str(), &o, &g_), ("cannot load " + text_path_).c_str());
+    else
+      Require(mce_graph_from_coo(u_.data(), v_.data(), u_.size(), &o, &g_), "graph build");
   }
   return g_;
 }
 
 void Graph::SortByOrder(OrderType order) {
-  if (!u_.empty() || !g_) {
+  if (!text_path_.empty() || !u_.empty() || !g_) {
     order_ = order;
     mce_graph_free(g_);
     g_ = nullptr;

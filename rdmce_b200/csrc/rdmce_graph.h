@@ -34,8 +34,8 @@ class Graph {
   Graph(Graph &&other) noexcept;
   ~Graph();
 
-  // COO text, src/graph.cc:64-152 (the edge list is kept on the host until
-  // SortByOrder / the first solve builds the device graph)
+  // COO text, src/graph.cc:64-152 (parsed on the GPU when SortByOrder or the
+  // first use builds the device graph)
   void LoadFromFile(const std::string &path);
   // the reference .bin container, already ordered (src/graph.cc:178-213)
   void LoadFromBin(const std::string &path);
@@ -63,6 +63,7 @@ class Graph {
   std::string name_;
   int device_ = 0;
   OrderType order_ = OrderType::DEG;
+  std::string text_path_;        // pending COO text file (parsed on the GPU at build)
   std::vector<uint32_t> u_, v_;  // pending COO pairs
   std::vector<uint32_t> rowoffset_, colidx_, labels_;
   mce_graph *g_ = nullptr;

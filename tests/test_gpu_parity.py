@@ -306,3 +306,21 @@ def test_deferred_roots_with_small_slabs(gpu, oracle_mod, heavy_warps):
         ocnt, ochk = og.mce_roots(roots, threads=THREADS)
         cnt, chk = g.solve_roots(roots, opts(gpu, **small))
     assert np.array_equal(cnt, ocnt) and np.array_equal(chk, ochk)
+
+
+def test_build_bytes_counter_matches_oracle(gpu, oracle_mod):
+    """The engine's count of algorithmic ego-network build bytes (the
+    roofline's traffic baseline, MCE_FLAG_STATS) equals the oracle's, root set
+    by root set, including a full solve with deferred roots."""
+    u, v = gpu.gen_rmat(15, 16, 2)
+    with gpu.Graph.from_coo(u, v, opts(gpu)) as g:
+        ro, ci, lab = g.export_csr()
+        og = oracle_mod.Graph.from_csr(ro.astype(np.uint64), ci, lab)
+        roots = np.sort(np.random.default_rng(3).choice(og.m, 500, replace=False)).astype(np.uint64)
+        _, _, o = og.mce_root_set(roots, threads=THREADS)
+        r = g.solve_root_list(roots, opts(gpu, flags=gpu.FLAG_STATS))
+        assert (r.count, r.checksum) == (o.count, o.checksum)
+        assert r.build_bytes == o.build_bytes > 0
+        full = g.solve(opts(gpu, flags=gpu.FLAG_STATS, slab_kib=16))
+        assert full.heavy_roots > 0
+        assert full.build_bytes == og.mce(threads=THREADS).build_bytes
