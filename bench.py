@@ -735,6 +735,65 @@ def serve_measure(args):
                    "requests' device-clock spans (mce_server_request_span)"}
 
 
+def run_ingest(args):
+    """Text ingest: the R-MAT scale-20 graph as 16.8M lines of COO text, loaded
+    (a) by the reference's own Graph::LoadFromFile text loop (its printed read
+    time, oracle/_ref/ref_cpu), (b) by the engine's parallel host parser, and
+    (c) on the GPU: file streamed to device memory, parsed there, pairs handed
+    to the device graph build (mce_graph_load_file).  (c) is timed through the
+    C ABI with host wall clock, the build included; its parse part is the
+    phase_ms[H2D] slot of the result."""
+    import numpy as np
+    import torch
+
+    import rdmce_b200 as mce
+
+    torch.cuda.set_device(0)
+    u, v = mce.gen_rmat(SCALE, EDGE_FACTOR, GRAPH_SEED)
+    o = mce.options(device=0)
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "rmat20.txt")
+        with open(path, "w") as f:
+            for i in range(0, len(u), 1 << 20):
+                blk = np.stack([u[i:i + (1 << 20)], v[i:i + (1 << 20)]], axis=1)
+                f.write("\n".join(f"{a} {b}" for a, b in blk.tolist()))
+                f.write("\n")
+        size = os.path.getsize(path)
+        ref_read = None
+        if os.path.exists(REF_CPU):
+            out = subprocess.run([REF_CPU, "stats", path], capture_output=True, text=True, timeout=900)
+            for line in out.stdout.splitlines():
+                if line.startswith("Read ") and " seconds" in line:
+                    ref_read = float(line.split(" in ")[1].split()[0])
+        for _ in range(args.warmup):
+            hu, hv = mce.parse_text(path)
+            gu, gv = mce.parse_text(path, device=0)
+            if not (np.array_equal(hu, u) and np.array_equal(gu, u) and np.array_equal(gv, v)):
+                raise RuntimeError("parsed pairs differ from the generator's")
+        host_s, gpu_parse_ms, load_s = [], [], []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            mce.parse_text(path)
+            host_s.append(time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            with mce.Graph.load_file(path, o) as g:
+                load_s.append(time.perf_counter() - t0)
+                r = g.solve_root_list(np.zeros(1, np.uint64), o)
+                gpu_parse_ms.append(r.phase_ms[mce.PHASE_H2D])
+    med = statistics.median
+    emit({"metric": "COO text ingest (file -> device graph)", "value": size / med(load_s) / 1e9, "unit": "GB/s",
+          "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+          "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+          "config": {"workload": f"R-MAT scale {SCALE}, edge factor {EDGE_FACTOR}, seed {GRAPH_SEED} as COO text",
+                     "bytes": size, "lines": int(len(u))},
+          "gpu_file_to_graph_s": med(load_s), "gpu_parse_incl_upload_ms": med(gpu_parse_ms),
+          "host_parse_s": med(host_s), "reference_read_s": ref_read,
+          "parity": "GPU and host parses equal the generator's pairs",
+          "how": "host wall clock; the GPU parse time includes reading the file into pinned memory and the "
+                 "uploads; the reference's read time is the one its loader prints"})
+    return 0
+
+
 def run_batch(args):
     line = batch_measure(args)
     emit({**line, "n_gpus": 1, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
@@ -774,7 +833,7 @@ def main():
                     help="the headline root sample of R-MAT scale 20, the R-MAT 24 + planted-clique sample, or a "
                          "smaller graph enumerated in full")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU oracle time bound (0 = skip)")
-    ap.add_argument("--mode", choices=["solve", "batch", "serve"], default="solve",
+    ap.add_argument("--mode", choices=["solve", "batch", "serve", "ingest"], default="solve",
                     help="solve: the headline; batch: many-instance graphs/s; serve: the request loop")
     ap.add_argument("--batch-graphs", type=int, default=10000)
     ap.add_argument("--plain-graphs", type=int, default=1000, help="graphs timed with one plain solve each")
@@ -795,6 +854,8 @@ def main():
         return run_batch(args)
     if args.mode == "serve":
         return run_serve(args)
+    if args.mode == "ingest":
+        return run_ingest(args)
     return run_ours(args)
 
 

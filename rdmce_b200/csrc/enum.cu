@@ -540,6 +540,60 @@ __device__ bool t0_spawn(const Ctx &c, const T0 &t, int level) {
   return true;
 }
 
+// Lanes whose index has bit k set: lane s stands for the subset s of a small
+// node's candidates (bit k = its k-th lowest candidate).
+__device__ __forceinline__ constexpr uint32_t lanes_with_bit(int k) {
+  return k == 0 ? 0xAAAAAAAAu : k == 1 ? 0xCCCCCCCCu : k == 2 ? 0xF0F0F0F0u : k == 3 ? 0xFF00FF00u : 0xFFFF0000u;
+}
+
+// A node with exactly N (3..5) candidates, decided in one step.  R + K is a
+// maximal clique for exactly the cliques K of the candidates that no active
+// row contains (a candidate outside K that extends K is itself such a row);
+// lane s tests the subset s.  Whether s is a clique is read off a warp-uniform
+// mask: each missing edge (i, j) excludes the lanes with bits i and j.  Rows
+// containing s: the AND of the per-candidate ballots over s's members.
+template <int N>
+__device__ __forceinline__ void t0_small_n(const Ctx &c, const T0 &t, uint32_t P, uint32_t A, uint32_t RM,
+                                           uint32_t &npend, uint64_t s10, uint64_t s20, uint32_t rsize0) {
+  WarpSmem *sm = c.sm;
+  const uint32_t lane = c.lane;
+  uint32_t qb[N], h[N], r[N - 1];
+  uint32_t pm = P;
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    qb[k] = pm & (0u - pm);
+    pm ^= qb[k];
+  }
+  // independent collectives: rows holding each candidate, the candidates' rows
+#pragma unroll
+  for (int k = 0; k < N; k++) h[k] = A & __ballot_sync(kFull, (t.row & qb[k]) != 0);
+#pragma unroll
+  for (int k = 0; k < N - 1; k++) r[k] = __shfl_sync(kFull, t.row, __ffs(qb[k]) - 1);
+  uint32_t notclique = 0;
+#pragma unroll
+  for (int i = 0; i < N - 1; i++)
+#pragma unroll
+    for (int j = i + 1; j < N; j++)
+      if (!(r[i] & qb[j])) notclique |= lanes_with_bit(i) & lanes_with_bit(j);
+  uint32_t rows = A, mask = RM;
+#pragma unroll
+  for (int k = 0; k < N; k++)
+    if ((lane >> k) & 1) {
+      rows &= h[k];
+      mask |= qb[k];
+    }
+  const bool out = lane != 0 && lane < (1u << N) && !((notclique >> lane) & 1) && rows == 0;
+  const uint32_t E = __ballot_sync(kFull, out);
+  const uint32_t pos = npend + __popc(E & lanemask_lt());
+  if (out && pos < 32) sm->pend_rm[pos] = mask;
+  npend += __popc(E);
+  if (npend >= 32) {
+    t0_flush(c, 32, s10, s20, rsize0);
+    if (out && pos >= 32) sm->pend_rm[pos - 32] = mask;
+    npend -= 32;
+  }
+}
+
 // A node with 1 to kSmallP candidates P, active rows A and R = RM, decided
 // in one step: its maximal cliques go to the pending leaves.
 __device__ __forceinline__ void t0_small(const Ctx &c, const T0 &t, uint32_t P, uint32_t A, uint32_t RM,
@@ -586,41 +640,10 @@ __device__ __forceinline__ void t0_small(const Ctx &c, const T0 &t, uint32_t P, 
       return;
     }
   }
-  {
-    // Few candidates: R + K is a maximal clique for exactly the cliques K of
-    // the candidates that no active row contains (a candidate outside K that
-    // extends K is itself such a row).  Lane i tests the i-th subset of P.
-    const uint32_t n = __popc(P);
-    uint32_t pm = P, qbit[kSmallP], adj[kSmallP], holds[kSmallP];
-#pragma unroll
-    for (int k = 0; k < kSmallP; k++) {
-      qbit[k] = pm & (0u - pm);
-      pm &= pm - 1;
-      adj[k] = qbit[k] ? (__shfl_sync(kFull, t.row, __ffs(qbit[k] | 0x80000000u) - 1) & P) : 0;
-      holds[k] = A & __ballot_sync(kFull, (t.row & qbit[k]) != 0);
-    }
-    uint32_t mask = 0, rows = ~0u;
-    bool clique = true;
-#pragma unroll
-    for (int k = 0; k < kSmallP; k++)
-      if ((lane >> k) & 1) {
-        mask |= qbit[k];
-        rows &= holds[k];
-      }
-#pragma unroll
-    for (int k = 0; k < kSmallP; k++)
-      if ((lane >> k) & 1) clique = clique && ((adj[k] & mask) == (mask & ~qbit[k]));
-    const bool out = lane != 0 && lane < (1u << n) && clique && rows == 0;
-    const uint32_t E = __ballot_sync(kFull, out);
-    const uint32_t pos = npend + __popc(E & lanemask_lt());
-    if (out && pos < 32) sm->pend_rm[pos] = RM | mask;
-    npend += __popc(E);
-    if (npend >= 32) {
-      t0_flush(c, 32, s10, s20, rsize0);
-      if (out && pos >= 32) sm->pend_rm[pos - 32] = RM | mask;
-      npend -= 32;
-    }
-    return;
+  switch (__popc(P)) {
+    case 3: t0_small_n<3>(c, t, P, A, RM, npend, s10, s20, rsize0); break;
+    case 4: t0_small_n<4>(c, t, P, A, RM, npend, s10, s20, rsize0); break;
+    default: t0_small_n<5>(c, t, P, A, RM, npend, s10, s20, rsize0); break;
   }
 }
 
@@ -693,17 +716,22 @@ expand:  // next candidate of VP at this level
     if (cand == 0) goto backtrack;
     const uint32_t q = __ffs(cand) - 1;
     P &= ~(1u << q);
+    // the child's candidates and the rows holding q: two independent
+    // collectives; rows holding R' = R + q (+ E) are A & those
     uint32_t P2 = P & __shfl_sync(kFull, t.row, q);
+    uint32_t A2 = A & __ballot_sync(kFull, (t.row >> q) & 1);
     uint32_t M = 1u << q;
     if (expand_r && (P2 & (P2 - 1))) {
       // EXPAND_R: a candidate adjacent to every other candidate joins R at
       // once; rows carry no self bit, so that is P2 \ row == {itself}
       const uint32_t E = __ballot_sync(kFull, (P2 & ~t.row) == lanebit);
       if (kStats) wops += 2 * __popc(P2);
-      P2 &= ~E;
-      M |= E;
+      if (E) {
+        P2 &= ~E;
+        M |= E;
+        A2 &= __ballot_sync(kFull, (t.row & E) == E);
+      }
     }
-    const uint32_t A2 = A & __ballot_sync(kFull, (t.row & M) == M);
     if (kStats) wops += __popc(A) + 1;
     if (P2 == 0) {  // leaf child: maximal iff no row contains R + M
       if (kStats) nodes++;
@@ -1815,7 +1843,7 @@ __device__ bool solve_root(const Ctx &c, uint64_t r) {
 
 // Solve a task popped from the pool; the block goes back to the free ring as
 // soon as its contents are in registers or in the slab.
-__device__ void solve_block(const Ctx &c, uint32_t blk) {
+__device__ __noinline__ void solve_block(Ctx c, uint32_t blk) {
   const EnumParams &P = *c.P;
   const char *rec = pool_block(P, blk);
   const uint32_t *hw = (const uint32_t *)rec;
@@ -1873,6 +1901,120 @@ __device__ void solve_block(const Ctx &c, uint32_t blk) {
   gen_solve(c, G, rsize, s1, s2);
 }
 
+// Root k of this solve's work list: solve it, or defer it to the
+// large-scratch pass (sized exactly), and record per-root values.  Not
+// inlined: the persistent loop around it then keeps almost nothing live.
+__device__ __noinline__ void run_root(Ctx c, uint64_t k) {
+  const EnumParams &P = *c.P;
+  WarpSmem *sm = c.sm;
+  // wk: the root's index in this solve's work list (per-root results are
+  // kept by it); the large-scratch pass walks a list of such indices
+  const uint64_t wk = P.heavy_list ? P.heavy_list[k] : k;
+  const uint64_t r = P.root_list ? P.root_list[wk] : P.re - 1 - wk;  // range: late-peeled roots first
+  const unsigned long long c0 = sm->count, h0 = sm->checksum;
+  const unsigned long long tr = now();
+  const bool fit = solve_root(c, r);
+  if (c.lane == 0) atomicMax(P.stat_max_item, now() - tr);
+  if (!fit) {
+    if (P.push_heavy) {
+      // defer the root, sized exactly: the slab must hold its candidate
+      // list and an ego network of p columns and up to nc rows
+      uint32_t nc = 0, nx = 0;
+      intersect_count(P.g, P.g.root_v0[r], P.g.root_v1[r], &nc, &nx);
+      if (c.lane == 0) {
+        const uint32_t slot = atomicAdd(P.heavy_n, 1u);
+        if (slot < P.heavy_cap) {
+          P.heavy_out[slot] = (uint32_t)wk;
+          const uint32_t p = nc - nx;
+          atomicMax(P.heavy_need, (unsigned long long)layout_for(nc, p, nc, (p + 63) / 64).need);
+        } else {
+          atomicExch(P.error, 4u);  // more deferred roots than the list holds
+        }
+      }
+    } else if (c.lane == 0) {
+      atomicExch(P.error, 2u);
+    }
+  }
+  if (P.per_root_count) {
+    // fold the per-lane checksums of batched leaves into this root's
+    const uint64_t lc = warp_sum_u64(sm->lchk[c.lane]);
+    sm->lchk[c.lane] = 0;
+    __syncwarp();
+    if (c.lane == 0) {
+      sm->checksum += lc;
+      if (fit) {  // a deferred root's values come from the large-scratch pass
+        P.per_root_count[wk] = sm->count - c0;
+        P.per_root_checksum[wk] = sm->checksum - h0;
+      }
+    }
+  }
+  __syncwarp();
+}
+
+// Wait for a task while other warps are busy.  Returns a pool block taken
+// from the ready queue (the warp then counts as busy), or -1 when no work is
+// left anywhere (or the wait's bound ran out: the error word says so).
+//
+// At most one warp per block polls the global queue at a time (the block's
+// poll token); the others sleep.  A warp counts itself busy only after it has
+// taken a task, so a failed attempt costs no atomic on the busy count.
+// Reading the busy count before the queue: a task is published before its
+// producer stops counting as busy, so "nobody busy" then "queue empty" means
+// no work is left -- except for a task taken between the two reads, whose
+// taker then finishes everything it exposes by itself if all others have
+// left.  Exit waits for two such observations a back-off apart, which makes
+// that case rare.  Not inlined, so its loop holds only a few values: idle
+// polling costs no reloads of the caller's state.
+__device__ __noinline__ int idle_wait(Ctx c, unsigned int *s_poll) {
+  const EnumParams &P = *c.P;
+  WarpSmem *sm = c.sm;
+  uint64_t idle_spins = 0;
+  uint32_t quiet = 0;  // consecutive "nobody busy, queue empty" observations
+  for (;;) {
+    int result = -2;  // -2: keep waiting
+    if (c.lane == 0) {
+      const unsigned long long ti0 = now();
+      bool polled = false, seen = false;
+      if (atomicCAS(s_poll, 0u, 1u) == 0u) {
+        polled = true;
+        const uint32_t act = *(volatile unsigned int *)P.active;
+        __threadfence();
+        const unsigned long long rh = *(volatile unsigned long long *)P.ready_head;
+        const unsigned long long rt = *(volatile unsigned long long *)P.ready_tail;
+        if (rh < rt) {
+          seen = true;
+          uint32_t b = 0;
+          if (ring_pop(P.ready_slot, P.ready_seq, P.ready_head, P.ready_tail, P.pool_mask, &b, P)) {
+            atomicAdd(P.active, 1u);
+            result = (int)b;
+          }
+          quiet = 0;
+        } else if (act == 0) {
+          if (++quiet >= 2) result = -1;
+        } else {
+          quiet = 0;
+        }
+        atomicExch(s_poll, 0u);
+      }
+      if (result == -2) {
+        if (++idle_spins > P.spin_limit) {
+          atomicExch(P.error, 1u);
+          result = -1;
+        } else if (!polled || seen) {
+          __nanosleep(500u + ((uint32_t)(clock64() >> 3) & 511u));
+        } else {
+          // back off, with jitter, so idle warps do not hammer the control words
+          const uint32_t shift = idle_spins < 6 ? (uint32_t)idle_spins : 6u;
+          __nanosleep((256u << shift) + ((uint32_t)(clock64() >> 3) & 1023u));
+        }
+      }
+      sm->cyc[kCycIdle] += now() - ti0;
+    }
+    result = __shfl_sync(kFull, result, 0);
+    if (result != -2) return result;
+  }
+}
+
 __global__ void __launch_bounds__(256, 4) k_enumerate(const __grid_constant__ EnumParams P) {
   extern __shared__ uint64_t smem_raw[];
   Ctx c;
@@ -1891,7 +2033,7 @@ __global__ void __launch_bounds__(256, 4) k_enumerate(const __grid_constant__ En
   if (c.lane == 0) {
     for (int i = 0; i < kCycPhases; i++) sm->cyc[i] = 0;
   }
-  __shared__ unsigned int s_poll;  // the block's poll token (see the idle loop)
+  __shared__ unsigned int s_poll;  // the block's poll token (see idle_wait)
   if (threadIdx.x == 0) s_poll = 0;
   __syncthreads();
   const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1901,141 +2043,48 @@ __global__ void __launch_bounds__(256, 4) k_enumerate(const __grid_constant__ En
   c.sharing = P.sharing != 0;
   const uint64_t total = P.heavy_list ? P.n_heavy : (P.root_list ? P.n_list : P.re - P.rb);
   unsigned long long nroots = 0;
-  bool roots_left = true;
-  uint64_t idle_spins = 0;
-  uint32_t quiet = 0;  // consecutive "nobody busy, queue empty" observations
   // a warp counts itself busy from its first root claim until a claim fails,
   // so warps that start late (not co-resident) are never waited for
   if (c.lane == 0) atomicAdd(P.active, 1u);
   __syncwarp();
   for (;;) {
-    if (roots_left) {
-      // queued tasks first: they are the open top of the heaviest subtrees
-      if (c.sharing) {
-        bool got = false;
-        uint32_t b = 0;
-        const unsigned long long tq = now();
-        if (c.lane == 0) got = ring_pop(P.ready_slot, P.ready_seq, P.ready_head, P.ready_tail, P.pool_mask, &b, P);
-        got = __shfl_sync(kFull, got, 0);
-        const uint32_t blk = __shfl_sync(kFull, b, 0);
-        if (c.lane == 0) sm->cyc[kCycQueue] += now() - tq;
-        if (got) {
-          const unsigned long long tb = now();
-          solve_block(c, blk);
-          if (c.lane == 0) atomicMax(P.stat_max_item + 1, now() - tb);
-          continue;
-        }
-      }
-      unsigned long long k = 0;
-      if (c.lane == 0) k = atomicAdd(P.next, 1ULL);
-      k = __shfl_sync(kFull, k, 0);
-      if (k < total) {
-        // wk: the root's index in this solve's work list (per-root results are
-        // kept by it); the large-scratch pass walks a list of such indices
-        const uint64_t wk = P.heavy_list ? P.heavy_list[k] : k;
-        const uint64_t r = P.root_list ? P.root_list[wk] : P.re - 1 - wk;  // range: late-peeled roots first
-        const unsigned long long c0 = sm->count, h0 = sm->checksum;
-        nroots++;
-        const unsigned long long tr = now();
-        const bool fit = solve_root(c, r);
-        if (c.lane == 0) atomicMax(P.stat_max_item, now() - tr);
-        if (!fit) {
-          if (P.push_heavy) {
-            // defer the root, sized exactly: the slab must hold its candidate
-            // list and an ego network of p columns and up to nc rows
-            uint32_t nc = 0, nx = 0;
-            intersect_count(P.g, P.g.root_v0[r], P.g.root_v1[r], &nc, &nx);
-            if (c.lane == 0) {
-              const uint32_t slot = atomicAdd(P.heavy_n, 1u);
-              if (slot < P.heavy_cap) {
-                P.heavy_out[slot] = (uint32_t)wk;
-                const uint32_t p = nc - nx;
-                atomicMax(P.heavy_need, (unsigned long long)layout_for(nc, p, nc, (p + 63) / 64).need);
-              } else {
-                atomicExch(P.error, 4u);  // more deferred roots than the list holds
-              }
-            }
-          } else if (c.lane == 0) {
-            atomicExch(P.error, 2u);
-          }
-        }
-        if (P.per_root_count) {
-          // fold the per-lane checksums of batched leaves into this root's
-          const uint64_t lc = warp_sum_u64(sm->lchk[c.lane]);
-          sm->lchk[c.lane] = 0;
-          __syncwarp();
-          if (c.lane == 0) {
-            sm->checksum += lc;
-            if (fit) {  // a deferred root's values come from the large-scratch pass
-              P.per_root_count[wk] = sm->count - c0;
-              P.per_root_checksum[wk] = sm->checksum - h0;
-            }
-          }
-        }
-        __syncwarp();
+    // queued tasks first: they are the open top of the heaviest subtrees
+    if (c.sharing) {
+      bool got = false;
+      uint32_t b = 0;
+      const unsigned long long tq = now();
+      if (c.lane == 0) got = ring_pop(P.ready_slot, P.ready_seq, P.ready_head, P.ready_tail, P.pool_mask, &b, P);
+      got = __shfl_sync(kFull, got, 0);
+      const uint32_t blk = __shfl_sync(kFull, b, 0);
+      if (c.lane == 0) sm->cyc[kCycQueue] += now() - tq;
+      if (got) {
+        const unsigned long long tb = now();
+        solve_block(c, blk);
+        if (c.lane == 0) atomicMax(P.stat_max_item + 1, now() - tb);
         continue;
       }
-      roots_left = false;
-      if (c.lane == 0) atomicSub(P.active, 1u);
-      if (!c.sharing) break;
     }
-    // Idle.  At most one warp per block polls the global queue at a time (the
-    // block's poll token); the others sleep.  A warp counts itself busy only
-    // after it has taken a task, so a failed attempt costs no atomic on the
-    // busy count.  Reading the busy count before the queue: a task is
-    // published before its producer stops counting as busy, so "nobody busy"
-    // then "queue empty" means no work is left -- except for a task taken
-    // between the two reads, whose taker then finishes everything it exposes
-    // by itself if all others have left.  Exit waits for two such
-    // observations a back-off apart, which makes that case rare.
-    bool done = false, got = false;
-    uint32_t b = 0;
-    const unsigned long long ti0 = now();
-    if (c.lane == 0) {
-      bool polled = false, seen = false;
-      if (atomicCAS(&s_poll, 0u, 1u) == 0u) {
-        polled = true;
-        const uint32_t act = *(volatile unsigned int *)P.active;
-        __threadfence();
-        const unsigned long long rh = *(volatile unsigned long long *)P.ready_head;
-        const unsigned long long rt = *(volatile unsigned long long *)P.ready_tail;
-        if (rh < rt) {
-          seen = true;
-          got = ring_pop(P.ready_slot, P.ready_seq, P.ready_head, P.ready_tail, P.pool_mask, &b, P);
-          if (got) atomicAdd(P.active, 1u);
-          quiet = 0;
-        } else if (act == 0) {
-          if (++quiet >= 2) done = true;
-        } else {
-          quiet = 0;
-        }
-        atomicExch(&s_poll, 0u);
-      }
-      if (!got && !done) {
-        if (++idle_spins > P.spin_limit) {
-          atomicExch(P.error, 1u);
-          done = true;
-        } else if (!polled || seen) {
-          __nanosleep(500u + ((uint32_t)(clock64() >> 3) & 511u));
-        } else {
-          // back off, with jitter, so idle warps do not hammer the control words
-          const uint32_t shift = idle_spins < 6 ? (uint32_t)idle_spins : 6u;
-          __nanosleep((256u << shift) + ((uint32_t)(clock64() >> 3) & 1023u));
-        }
-      }
-      sm->cyc[kCycIdle] += now() - ti0;
-    }
-    got = __shfl_sync(kFull, got, 0);
-    if (got) {
+    unsigned long long k = 0;
+    if (c.lane == 0) k = atomicAdd(P.next, 1ULL);
+    k = __shfl_sync(kFull, k, 0);
+    if (k >= total) break;
+    nroots++;
+    run_root(c, k);
+  }
+  if (c.lane == 0) atomicSub(P.active, 1u);
+  if (c.sharing) {
+    // roots are gone: take tasks until no warp has work left
+    for (;;) {
+      const int blk = idle_wait(c, &s_poll);
+      if (blk < 0) break;
       const unsigned long long tb = now();
-      solve_block(c, __shfl_sync(kFull, b, 0));
-      if (c.lane == 0) atomicMax(P.stat_max_item + 1, now() - tb);
-      if (c.lane == 0) atomicSub(P.active, 1u);
-      idle_spins = 0;
-      quiet = 0;
-      continue;
+      solve_block(c, (uint32_t)blk);
+      if (c.lane == 0) {
+        atomicMax(P.stat_max_item + 1, now() - tb);
+        atomicSub(P.active, 1u);
+      }
+      __syncwarp();
     }
-    if (__shfl_sync(kFull, done, 0)) break;
   }
   acc_flush(c);
   if (c.lane == 0) {
