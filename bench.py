@@ -379,9 +379,12 @@ def run_ours(args):
         return r, e0.elapsed_time(e1)
 
     ref = None
+    trials = []  # the autotuner's trials of the kernel builds (blocks per SM, device ms)
     for _ in range(args.warmup):
         r, _ms = step()
         ref = (r.count, r.checksum)
+        if r.autotune == 1:
+            trials.append([r.blocks_per_sm, round(r.phase_ms[mce.PHASE_ENUMERATE], 3)])
     # parity: the headline sample must reproduce the CPU oracle's fixture
     fx = None
     parity = "self-consistent across steps (no fixture)"
@@ -414,8 +417,10 @@ def run_ours(args):
     times, enum_ms, launches_enum = [], 0.0, 0
     cycles = [0] * 6
     cliques = 0
+    used = set()
     for _ in range(args.steps):
         r, ms = step()
+        used.add((r.blocks_per_sm, r.autotune))
         if ref is not None and (r.count, r.checksum) != ref:
             raise RuntimeError(f"nondeterministic result: {(r.count, r.checksum)} vs {ref}")
         ref = (r.count, r.checksum)
@@ -516,6 +521,10 @@ def run_ours(args):
                     "graph_build_ms_per_step": sum(pre_ms[1:]) / max(1, len(pre_ms) - 1),
                     "how": "host wall clock around mce_graph_from_coo (pinned host COO in) + mce_solve_root_list "
                            "(result struct out), on the engine's own stream"},
+            "autotune": {"trials": trials, "timed_steps": sorted(used),
+                         "how": "blocks_per_sm = 0: the first solves of the workload try 4, 5 and 3 resident "
+                                "8-warp blocks per SM (64, 51, 85 registers a thread), later solves use the "
+                                "fastest; [blocks per SM, mode] of the timed steps, mode 2 = the tuner's choice"},
             "gpu_launches": int(launches),
             "clocks": clk,
             "search": {"nodes_per_step": int(nodes), "word_ops_per_step": int(wops),

@@ -64,8 +64,12 @@ typedef enum mce_order { MCE_ORDER_DEGENERACY = 0, MCE_ORDER_UNCHANGED = 1, MCE_
 typedef struct mce_options {
   int device;                 /* CUDA ordinal (default 0) */
   int order;                  /* mce_order (default degeneracy) */
-  uint32_t warps_per_block;   /* 0 = autotuned */
-  uint32_t blocks_per_sm;     /* 0 = autotuned */
+  uint32_t warps_per_block;   /* warps per block (<= 8); 0 = 8 */
+  uint32_t blocks_per_sm;     /* resident 8-warp blocks per SM, 1..5, which also picks the kernel's
+                                 register budget (3: 85, 4: 64, 5: 51 registers a thread).
+                                 0 = autotuned: per graph and per workload (root range or root
+                                 list, flags), the first three solves run 4, 5 and 3 blocks per
+                                 SM in turn, timing each; later solves use the fastest. */
   uint32_t share_bound;       /* task-share bound tau; 0 = 24 (BkPivotBitBalance.cuh:6-8) */
   int expand_r;               /* aggressive node generation (mce_gpu.cuh:5); default 1 */
   uint64_t root_begin;        /* enumerate roots [root_begin, root_end); 0,0 = all roots */
@@ -92,6 +96,9 @@ typedef struct mce_result {
   uint32_t degeneracy;
   uint32_t max_degree;
   uint32_t status_detail;     /* nonzero: device error word (see mce_status_str) */
+  uint32_t blocks_per_sm;     /* resident 8-warp blocks per SM the enumeration ran with */
+  uint32_t autotune;          /* 0: blocks_per_sm was set by the caller; 1: the autotuner was
+                                 trying this setting; 2: the autotuner's choice */
   uint64_t num_vertices;      /* non-isolated vertices */
   uint64_t num_edges;         /* undirected simple edges */
   uint64_t roots;             /* roots enumerated */

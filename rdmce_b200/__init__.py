@@ -68,6 +68,8 @@ class _Result(C.Structure):
         ("degeneracy", C.c_uint32),
         ("max_degree", C.c_uint32),
         ("status_detail", C.c_uint32),
+        ("blocks_per_sm", C.c_uint32),
+        ("autotune", C.c_uint32),
         ("num_vertices", C.c_uint64),
         ("num_edges", C.c_uint64),
         ("roots", C.c_uint64),
@@ -134,13 +136,16 @@ class Result:
     warp_cycles: list = field(default_factory=list)
     max_item_cycles: list = field(default_factory=list)
     build_bytes: int = 0
+    blocks_per_sm: int = 0
+    autotune: int = 0
 
     @classmethod
     def _from(cls, r: _Result) -> "Result":
         hist = {s: int(r.hist[s]) for s in range(HIST_LEN) if r.hist[s]}
         return cls(r.count, r.checksum, hist, r.max_size, r.degeneracy, r.max_degree, r.num_vertices,
                    r.num_edges, r.roots, r.shared_tasks, r.heavy_roots, list(r.phase_ms), r.nodes, r.word_ops,
-                   r.launches, list(r.warp_cycles), list(r.max_item_cycles), r.build_bytes)
+                   r.launches, list(r.warp_cycles), list(r.max_item_cycles), r.build_bytes, r.blocks_per_sm,
+                   r.autotune)
 
 
 _lib = None

@@ -7,6 +7,7 @@
 #include <chrono>
 #include <cstring>
 #include <mutex>
+#include <unordered_map>
 #include <vector>
 
 #include "common.cuh"
@@ -22,6 +23,28 @@ struct mce_graph {
 };
 
 namespace mce {
+
+// The graph builders allocate their sort buffers stream-ordered
+// (cudaMallocAsync) from the device's default pool, whose release threshold
+// is 0: at every synchronisation the freed memory goes back to the driver and
+// the next build maps gigabytes again, which costs more than the build.  The
+// first time this process uses a device, its default pool is told to keep
+// freed memory for reuse (an attribute of this process's pool; it ends with
+// the process).
+void keep_pool_memory(int device) {
+  static std::mutex mu;
+  static std::vector<bool> done;
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)done.size() <= device) done.resize(device + 1, false);
+  if (done[device]) return;
+  done[device] = true;
+  cudaMemPool_t pool = nullptr;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+}
 
 namespace {
 
@@ -52,6 +75,7 @@ mce_status set_device(int device) {
   }
   if (device < 0 || device >= count) return MCE_ERR_INVALID_ARG;
   MCE_CUDA_TRY(cudaSetDevice(device));
+  keep_pool_memory(device);
   return MCE_OK;
 }
 
@@ -354,8 +378,51 @@ void mce_graph_free(mce_graph *g) {
   destroy_handle(g);
 }
 
+namespace mce {
+namespace {
+
+// A workload: which roots, and the settings that change the search.
+uint64_t workload_key(const mce_options &o, const uint64_t *roots_h, uint64_t n_roots, bool per_root) {
+  uint64_t k = mix64(o.root_begin) ^ mix64(o.root_end + 0x51ULL) ^ mix64(n_roots + 0x77ULL);
+  for (uint64_t i = 0; i < n_roots; i++) k = mix64(k ^ roots_h[i]);
+  k ^= mix64(((uint64_t)o.flags << 32) | ((uint64_t)o.expand_r << 8) | (per_root ? 1 : 0));
+  k ^= mix64(((uint64_t)o.share_bound << 32) | o.reg_share_bound) ^ mix64(((uint64_t)o.warps_per_block << 32) |
+                                                                          o.slab_kib);
+  return k;
+}
+
+// The autotuner's records, process-wide: keyed by the graph's fingerprint
+// (device, n, m, degeneracy, max degree) and the workload, so a graph built
+// again from the same input (as each end-to-end call does) keeps its tuning.
+std::mutex g_tune_mu;
+std::unordered_map<uint64_t, TuneRecord> g_tune;
+
+uint64_t tune_key(const mce_graph *g, uint64_t wkey) {
+  return mix64(wkey ^ mix64(((uint64_t)g->device << 48) ^ g->g.n)) ^ mix64(g->g.m + 0x1234567ULL) ^
+         mix64(((uint64_t)g->g.degeneracy << 32) | g->g.max_degree);
+}
+
+uint32_t tuned_blocks(mce_graph *g, uint64_t wkey, const mce_options &o, uint32_t *mode) {
+  if (o.blocks_per_sm) {
+    *mode = 0;
+    return o.blocks_per_sm;
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  return tune_pick(g_tune[tune_key(g, wkey)], (o.flags & MCE_FLAG_STATS) != 0, mode);
+}
+
+void record_tune(mce_graph *g, uint64_t wkey, uint32_t blocks, uint32_t mode, float ms) {
+  if (mode != 1) return;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  tune_record(g_tune[tune_key(g, wkey)], blocks, ms);
+}
+
+}  // namespace
+}  // namespace mce
+
 static mce_status solve_impl(mce_graph *g, const mce_options &o, mce_result *out, const uint64_t *roots_d,
-                             uint64_t n_roots, unsigned long long *cnt_d, unsigned long long *chk_d) {
+                             uint64_t n_roots, unsigned long long *cnt_d, unsigned long long *chk_d,
+                             uint64_t wkey) {
   MCE_CUDA_TRY(cudaSetDevice(g->device));
   std::memset(out, 0, sizeof(*out));
   Timer t;
@@ -372,6 +439,8 @@ static mce_status solve_impl(mce_graph *g, const mce_options &o, mce_result *out
   if (!res) return s;
   MCE_CUDA_TRY(cudaMemsetAsync(res, 0, res_bytes, st));
   EnumConfig cfg = config_from_options(o);
+  uint32_t tune_mode = 0;
+  cfg.blocks_per_sm = tuned_blocks(g, wkey, o, &tune_mode);
   cfg.spin_limit = spin_of(o);
   cfg.root_list = roots_d;
   cfg.n_root_list = n_roots;
@@ -382,6 +451,9 @@ static mce_status solve_impl(mce_graph *g, const mce_options &o, mce_result *out
   unsigned long long *hist = (unsigned long long *)(res + sizeof(SlotResult));
   s = enumerate(g->g, cfg, scr, st, slot, hist, &stats);
   if (s != MCE_OK) return s;
+  record_tune(g, wkey, cfg.blocks_per_sm, tune_mode, stats.ms_enum);
+  out->blocks_per_sm = stats.blocks_per_sm;
+  out->autotune = tune_mode;
   Timer t2;
   SlotResult hs;
   MCE_CUDA_TRY(cudaMemcpyAsync(&hs, slot, sizeof(hs), cudaMemcpyDeviceToHost, st));
@@ -416,7 +488,7 @@ mce_status mce_solve(mce_graph *g, const mce_options *opt, mce_result *out) {
   if (!g || !out) return MCE_ERR_INVALID_ARG;
   mce_options tmp;
   const mce_options &o = opts_or_default(opt, tmp);
-  return solve_impl(g, o, out, nullptr, 0, nullptr, nullptr);
+  return solve_impl(g, o, out, nullptr, 0, nullptr, nullptr, workload_key(o, nullptr, 0, false));
 }
 
 mce_status mce_solve_roots(mce_graph *g, const uint64_t *roots, uint64_t n_roots, const mce_options *opt,
@@ -445,7 +517,7 @@ mce_status mce_solve_roots(mce_graph *g, const uint64_t *roots, uint64_t n_roots
   }
   mce_options o2 = o;
   o2.flags |= MCE_FLAG_NO_SHARING;  // a root's cliques must stay with the warp that owns it
-  if (s == MCE_OK) s = solve_impl(g, o2, r, rd, n_roots, cd, hd);
+  if (s == MCE_OK) s = solve_impl(g, o2, r, rd, n_roots, cd, hd, workload_key(o2, roots, n_roots, true));
   if (s == MCE_OK) {
     if (cudaMemcpyAsync(counts, cd, n_roots * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaMemcpyAsync(checksums, hd, n_roots * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
@@ -475,7 +547,7 @@ mce_status mce_solve_root_list(mce_graph *g, const uint64_t *roots, uint64_t n_r
   mce_status s = MCE_OK;
   if (n_roots && cudaMemcpyAsync(rd, roots, n_roots * 8, cudaMemcpyHostToDevice, st) != cudaSuccess)
     s = MCE_ERR_CUDA;
-  if (s == MCE_OK) s = solve_impl(g, o, out, rd, n_roots, nullptr, nullptr);
+  if (s == MCE_OK) s = solve_impl(g, o, out, rd, n_roots, nullptr, nullptr, workload_key(o, roots, n_roots, false));
   cudaFreeAsync(rd, st);
   cudaStreamSynchronize(st);
   return s;

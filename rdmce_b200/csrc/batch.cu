@@ -27,6 +27,8 @@ struct mce_batch {
   // captured launch
   cudaGraphExec_t exec = nullptr;
   mce::EnumConfig exec_cfg;  // the settings the captured launch was planned with
+  mce::TuneRecord tune;      // the autotuner's timings of the kernel builds for this batch
+  uint32_t tune_mode = 0;    // how the captured launch's blocks per SM were chosen
   mce::EnumPlan plan;
   mce::SlotResult *slots_h = nullptr;  // pinned
   unsigned long long *hist_h = nullptr;
@@ -117,6 +119,7 @@ mce_status mce_batch_create(const uint32_t *u, const uint32_t *v, const uint64_t
     return MCE_ERR_NO_DEVICE;
   }
   MCE_CUDA_TRY(cudaSetDevice(o.device));
+  keep_pool_memory(o.device);
   mce_batch *b = new (std::nothrow) mce_batch();
   if (!b) return MCE_ERR_OUT_OF_MEMORY;
   b->device = o.device;
@@ -222,6 +225,10 @@ mce_status mce_batch_solve(mce_batch *b, const mce_options *opt, mce_batch_graph
   cfg.root_begin = cfg.root_end = 0;
   cfg.n_slots = ng;
   cfg.hist_len = hl;
+  // the autotuner (o.blocks_per_sm == 0): successive solves of the batch try
+  // the kernel builds in turn, then keep the fastest (each change re-captures)
+  uint32_t tune_mode = 0;
+  if (!o.blocks_per_sm) cfg.blocks_per_sm = tune_pick(b->tune, (o.flags & MCE_FLAG_STATS) != 0, &tune_mode);
   const bool rebuild = !b->exec || !same_plan_settings(cfg, b->exec_cfg);
   if (rebuild) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
@@ -277,6 +284,7 @@ mce_status mce_batch_solve(mce_batch *b, const mce_options *opt, mce_batch_graph
   cudaEventDestroy(e1);
   if (enumerate_ms) *enumerate_ms = ms;
   if (s != MCE_OK) return s;
+  if (tune_mode == 1) tune_record(b->tune, cfg.blocks_per_sm, ms);
   for (uint32_t i = 0; i < ng; i++) {
     results[i].count = b->slots_h[i].count;
     results[i].checksum = b->slots_h[i].checksum;

@@ -38,6 +38,9 @@ mce_status build_from_csr(uint64_t n, const uint32_t *off_d, const uint32_t *adj
 mce_status csr_to_edges(uint64_t n, const uint32_t *off, const uint32_t *adj, uint64_t m, uint32_t *deg,
                         uint32_t **eu, uint32_t **ev, cudaStream_t st);
 void free_graph(DeviceGraph *g);
+// first use of a device in this process: its default stream-ordered memory
+// pool keeps freed memory for reuse instead of returning it at every sync
+void keep_pool_memory(int device);
 // COO text file -> pairs in device memory (ingest.cu), with the reference
 // parser's semantics; *u_out / *v_out are cudaMallocAsync'ed on st (free with
 // cudaFreeAsync)
@@ -103,6 +106,7 @@ struct EnumStats {
   uint32_t error = 0;
   float ms_setup = 0, ms_enum = 0;
   uint64_t launches = 0;
+  uint32_t blocks_per_sm = 0;  // resident 8-warp blocks per SM the solve ran with
 };
 
 // Per-slot results written by the enumeration kernels.
@@ -173,6 +177,8 @@ struct EnumPlan {
   bool fits_all = false;  // every root fits the normal slab: no deferred pass possible
   uint32_t pool_blocks = 0;
   uint32_t heavy_warps = 0;  // cap on the large-scratch pass (0 = as memory allows)
+  int build = 4;             // which register-budget build of the kernel (enum_dispatch.cu)
+  uint32_t sms = 0;          // multiprocessors of the device
   void *ctl = nullptr;
   Scratch *scr = nullptr;
 };
@@ -185,6 +191,30 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
                      unsigned long long *hist, EnumPlan *plan);
 mce_status enum_launch(const EnumPlan &plan, cudaStream_t st);
 mce_status enum_finish(const EnumPlan &plan, cudaStream_t st, EnumStats *stats);
+// the kernel build a blocks_per_sm setting runs (0 = the default build)
+int enum_build_for(uint32_t blocks_per_sm);
+
+// The autotuner's record for one workload: the enumeration time of each
+// kernel build (3, 4, 5 blocks of 8 warps per SM), -1 while untried.  Solves
+// of the workload try the builds in turn (4, 5, 3); later ones use the
+// fastest.  A counting solve (MCE_FLAG_STATS, a slower kernel instance) is
+// never a trial.
+struct TuneRecord {
+  float ms[3] = {-1.f, -1.f, -1.f};
+};
+// blocks per SM for the next solve; *mode = 1 for a trial, 2 for the choice
+uint32_t tune_pick(const TuneRecord &t, bool counting, uint32_t *mode);
+void tune_record(TuneRecord &t, uint32_t blocks_per_sm, float ms);
+// the three register-budget builds of enum.cu (3, 4, 5 blocks of 8 warps per SM)
+#define MCE_DECLARE_ENUM_BUILD(b)                                                                         \
+  mce_status enum_plan_b##b(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, SlotResult *slots, \
+                            unsigned long long *hist, EnumPlan *plan);                                    \
+  mce_status enum_launch_b##b(const EnumPlan &plan, cudaStream_t st);                                     \
+  mce_status enum_finish_b##b(const EnumPlan &plan, cudaStream_t st, EnumStats *stats);
+MCE_DECLARE_ENUM_BUILD(3)
+MCE_DECLARE_ENUM_BUILD(4)
+MCE_DECLARE_ENUM_BUILD(5)
+#undef MCE_DECLARE_ENUM_BUILD
 mce_status probe_int_peak(int device, double *word_ops_per_s);
 
 }  // namespace mce

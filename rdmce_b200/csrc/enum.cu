@@ -49,6 +49,18 @@
 #include "common.cuh"
 #include "engine.h"
 
+// This file is compiled once per register budget of the enumeration kernel:
+// MCE_ENUM_BPS resident 8-warp blocks per SM (3, 4 or 5: at most 85, 64 or 51
+// registers a thread).  Each build keeps its own copies of the device
+// functions, so one budget never forces spills on another; enum_dispatch.cu
+// picks the build per solve (the autotuner's occupancy choice).
+#ifndef MCE_ENUM_BPS
+#define MCE_ENUM_BPS 4
+#endif
+#define MCE_CAT2(a, b) a##b
+#define MCE_CAT(a, b) MCE_CAT2(a, b)
+#define MCE_ENUM_FN(name) MCE_CAT(name, MCE_CAT(_b, MCE_ENUM_BPS))
+
 namespace mce {
 
 namespace {
@@ -749,8 +761,12 @@ expand:  // next candidate of VP at this level
       t0_small(c, t, P2, A2, RM | M, npend, s10, s20, rsize0);
       goto expand;
     }
-    sm->t0f[level] = make_uint4(P, VP, A, RM);
-    level++;
+    // a child that is its parent's last open candidate replaces the parent
+    // (no frame: the parent would only backtrack after it)
+    if (cand & (cand - 1)) {
+      sm->t0f[level] = make_uint4(P, VP, A, RM);
+      level++;
+    }
     P = P2;
     A = A2;
     RM |= M;
@@ -2015,7 +2031,7 @@ __device__ __noinline__ int idle_wait(Ctx c, unsigned int *s_poll) {
   }
 }
 
-__global__ void __launch_bounds__(256, 4) k_enumerate(const __grid_constant__ EnumParams P) {
+__global__ void __launch_bounds__(256, MCE_ENUM_BPS) k_enumerate(const __grid_constant__ EnumParams P) {
   extern __shared__ uint64_t smem_raw[];
   Ctx c;
   c.P = &P;
@@ -2137,32 +2153,15 @@ mce_status reset_ctl(const EnumPlan &plan, cudaStream_t st) {
   return MCE_OK;
 }
 
-// Integer-pipe probe: per thread, 8 independent chains of the enumeration's
-// word-op mix (a 64-bit ANDN feeding a 64-bit POPC, folded back by an add).
-__global__ void k_int_probe(const uint64_t *seed, uint64_t *sink, int iters) {
-  uint64_t a[8];
-  const uint64_t b = seed[0] ^ (threadIdx.x * 0x9E3779B97F4A7C15ULL);
-#pragma unroll
-  for (int i = 0; i < 8; i++) a[i] = seed[1] + (uint64_t)i * 0x632BE59BD9B4E019ULL + blockIdx.x;
-  for (int it = 0; it < iters; it++) {
-#pragma unroll
-    for (int i = 0; i < 8; i++) a[i] += __popcll(a[i] & ~b) | (a[i] << 7);
-  }
-  uint64_t x = 0;
-#pragma unroll
-  for (int i = 0; i < 8; i++) x ^= a[i];
-  if (x == 0x123456789ULL) sink[0] = x;  // keeps the chains live
-}
-
 }  // namespace
 
-mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, SlotResult *slots,
+mce_status MCE_ENUM_FN(enum_plan)(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, SlotResult *slots,
                      unsigned long long *hist, EnumPlan *plan) {
   const int device = scr->device;
   int sms = 0;
   MCE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
   const uint32_t wpb = cfg.warps_per_block ? std::min(cfg.warps_per_block, 8u) : 8u;
-  const uint32_t bps = cfg.blocks_per_sm ? std::min(cfg.blocks_per_sm, 4u) : 4u;
+  const uint32_t bps = cfg.blocks_per_sm ? std::min<uint32_t>(cfg.blocks_per_sm, MCE_ENUM_BPS) : MCE_ENUM_BPS;
   EnumParams &P = plan->params;
   P = EnumParams{};
   P.g.n = g.n;
@@ -2273,6 +2272,7 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
   P.push_heavy = 1;
   plan->heavy_warps = cfg.heavy_warps;
   plan->blocks = blocks;
+  plan->sms = (uint32_t)sms;
   plan->threads = wpb * 32;
   plan->smem = (size_t)wpb * sizeof(WarpSmem);
   plan->nwarps = nwarps;
@@ -2282,7 +2282,7 @@ mce_status enum_plan(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
   return MCE_OK;
 }
 
-mce_status enum_launch(const EnumPlan &plan, cudaStream_t st) {
+mce_status MCE_ENUM_FN(enum_launch)(const EnumPlan &plan, cudaStream_t st) {
   MCE_TRY(reset_ctl(plan, st));
   if (plan.nwork) {
     k_enumerate<<<plan.blocks, plan.threads, plan.smem, st>>>(plan.params);
@@ -2292,7 +2292,7 @@ mce_status enum_launch(const EnumPlan &plan, cudaStream_t st) {
   return MCE_OK;
 }
 
-mce_status enum_finish(const EnumPlan &plan, cudaStream_t st, EnumStats *stats) {
+mce_status MCE_ENUM_FN(enum_finish)(const EnumPlan &plan, cudaStream_t st, EnumStats *stats) {
   EnumCtl *ctl = (EnumCtl *)plan.ctl;
   EnumCtl h{};
   MCE_CUDA_TRY(cudaMemcpyAsync(&h, ctl, sizeof(EnumCtl), cudaMemcpyDeviceToHost, st));
@@ -2372,25 +2372,26 @@ mce_status enum_finish(const EnumPlan &plan, cudaStream_t st, EnumStats *stats) 
   return MCE_OK;
 }
 
-mce_status enumerate(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, cudaStream_t st, SlotResult *slots,
-                     unsigned long long *hist, EnumStats *stats) {
-  EnumPlan plan;
-  MCE_TRY(enum_plan(g, cfg, scr, slots, hist, &plan));
-  cudaEvent_t e0, e1;
-  MCE_CUDA_TRY(cudaEventCreate(&e0));
-  MCE_CUDA_TRY(cudaEventCreate(&e1));
-  cudaEventRecord(e0, st);
-  mce_status s = enum_launch(plan, st);
-  if (s == MCE_OK) s = enum_finish(plan, st, stats);
-  cudaEventRecord(e1, st);
-  cudaEventSynchronize(e1);
-  float ms = 0;
-  cudaEventElapsedTime(&ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  if (stats) stats->ms_enum = ms;
-  return s;
+#if MCE_ENUM_BPS == 4
+namespace {
+// Integer-pipe probe: per thread, 8 independent chains of the enumeration's
+// word-op mix (a 64-bit ANDN feeding a 64-bit POPC, folded back by an add).
+__global__ void k_int_probe(const uint64_t *seed, uint64_t *sink, int iters) {
+  uint64_t a[8];
+  const uint64_t b = seed[0] ^ (threadIdx.x * 0x9E3779B97F4A7C15ULL);
+#pragma unroll
+  for (int i = 0; i < 8; i++) a[i] = seed[1] + (uint64_t)i * 0x632BE59BD9B4E019ULL + blockIdx.x;
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) a[i] += __popcll(a[i] & ~b) | (a[i] << 7);
+  }
+  uint64_t x = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) x ^= a[i];
+  if (x == 0x123456789ULL) sink[0] = x;  // keeps the chains live
 }
+
+}  // namespace
 
 mce_status probe_int_peak(int device, double *word_ops_per_s) {
   MCE_CUDA_TRY(cudaSetDevice(device));
@@ -2420,5 +2421,7 @@ mce_status probe_int_peak(int device, double *word_ops_per_s) {
   *word_ops_per_s = 2.0 * 8.0 * iters * (double)threads * blocks / (ms * 1e-3);
   return MCE_OK;
 }
+
+#endif
 
 }  // namespace mce

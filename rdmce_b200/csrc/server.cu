@@ -217,6 +217,7 @@ mce_status mce_server_create(const mce_server_options *opt, mce_server **out) {
   }
   if (o.device < 0 || o.device >= count) return MCE_ERR_INVALID_ARG;
   MCE_CUDA_TRY(cudaSetDevice(o.device));
+  mce::keep_pool_memory(o.device);
   size_t freeb = 0, totalb = 0;
   MCE_CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
   mce_server *s = new (std::nothrow) mce_server();

@@ -324,3 +324,37 @@ def test_build_bytes_counter_matches_oracle(gpu, oracle_mod):
         full = g.solve(opts(gpu, flags=gpu.FLAG_STATS, slab_kib=16))
         assert full.heavy_roots > 0
         assert full.build_bytes == og.mce(threads=THREADS).build_bytes
+
+
+def test_autotuner_tries_each_build_then_keeps_one(gpu, oracle_mod):
+    """blocks_per_sm = 0: the first three solves of a workload run the 4-, 5-
+    and 3-blocks-per-SM builds (64, 51, 85 registers a thread), later ones the
+    fastest of them; every build gives the same cliques.  An explicit setting
+    is used as given."""
+    u, v = gpu.gen_rmat(13, 16, 6)
+    _, o = oracle_result(oracle_mod, u, v)
+    with gpu.Graph.from_coo(u, v, opts(gpu)) as g:
+        runs = [g.solve(opts(gpu)) for _ in range(5)]
+        for r in runs:
+            assert_same(r, o, f"blocks per SM {r.blocks_per_sm}")
+        assert [(r.blocks_per_sm, r.autotune) for r in runs[:3]] == [(4, 1), (5, 1), (3, 1)]
+        assert runs[3].autotune == runs[4].autotune == 2
+        assert runs[3].blocks_per_sm == runs[4].blocks_per_sm in (3, 4, 5)
+        # a different workload (a root range) is tuned on its own
+        part = g.solve(opts(gpu, root_begin=0, root_end=1000))
+        assert (part.blocks_per_sm, part.autotune) == (4, 1)
+        for b in (1, 2, 3, 4, 5):
+            r = g.solve(opts(gpu, blocks_per_sm=b))
+            assert (r.blocks_per_sm, r.autotune) == (b, 0)
+            assert_same(r, o, f"explicit {b}")
+
+
+def test_batch_autotuner_recaptures(gpu, oracle_mod):
+    graphs = [gpu.gen_batch_member(i)[:2] for i in range(40)]
+    b = gpu.Batch(graphs, opts(gpu))
+    try:
+        outs = [b.solve(opts(gpu))[:2] for _ in range(5)]
+    finally:
+        b.close()
+    for res, hist in outs[1:]:
+        assert res == outs[0][0] and np.array_equal(hist, outs[0][1])
