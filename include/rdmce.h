@@ -247,7 +247,7 @@ typedef struct mce_server mce_server;
 typedef struct mce_server_options {
   int device;
   uint64_t memory_budget;     /* bytes of device memory admissions may use; 0 = 60% of free */
-  uint32_t max_inflight;      /* concurrent requests on the device; 0 = 8 */
+  uint32_t max_inflight;      /* requests on the device at once, across the admitted batches; 0 = 256 */
   uint32_t reserved[5];
 } mce_server_options;
 

@@ -20,7 +20,6 @@ struct mce_batch {
   cudaStream_t stream = nullptr;
   mce::DeviceGraph g;
   uint32_t n_graphs = 0;
-  uint32_t *label_base = nullptr;  // device, n_graphs + 1
   std::vector<uint32_t> nv;
   std::vector<uint64_t> ne;
   mce::Scratch scr;
@@ -94,7 +93,98 @@ __global__ void k_count_per_graph(const uint32_t *slot, uint32_t n, const uint32
   }
 }
 
+// Per graph: largest degree and largest number of later neighbours.  In the
+// union's degeneracy order each graph's vertices keep its own peel order (the
+// graphs never interact), so the largest later-neighbour count of a graph's
+// vertices is that graph's degeneracy.
+__global__ void k_graph_degrees(const uint32_t *off, const uint32_t *adj, uint32_t n, const uint32_t *slot,
+                                unsigned int *maxdeg, unsigned int *degen) {
+  for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < n; x += gridDim.x * blockDim.x) {
+    const uint32_t b = off[x], e = off[x + 1];
+    uint32_t lo = b, hi = e;  // first neighbour above x
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (adj[mid] <= x) lo = mid + 1;
+      else hi = mid;
+    }
+    atomicMax(&maxdeg[slot[x]], e - b);
+    atomicMax(&degen[slot[x]], e - lo);
+  }
+}
+
 }  // namespace
+
+mce_status build_union(uint32_t *ud, uint32_t *vd, const uint64_t *pair_offsets, uint32_t n_graphs, int order,
+                       uint64_t spin_limit, cudaStream_t st, DeviceGraph *g, UnionCounts *counts) {
+  const uint64_t np = pair_offsets[n_graphs];
+  uint32_t *gmax = nullptr, *base = nullptr;
+  uint64_t *pd = nullptr;
+  struct Free {
+    cudaStream_t st;
+    std::vector<void *> p;
+    ~Free() {
+      for (void *q : p)
+        if (q) cudaFreeAsync(q, st);
+    }
+  } fr{st, {}};
+  if (cudaMallocAsync(&pd, (n_graphs + 1) * 8ULL, st) != cudaSuccess ||
+      cudaMallocAsync(&gmax, (n_graphs + 1) * 4ULL, st) != cudaSuccess ||
+      cudaMallocAsync(&base, (n_graphs + 1) * 4ULL, st) != cudaSuccess)
+    return MCE_ERR_OUT_OF_MEMORY;
+  fr.p = {pd, gmax, base};
+  MCE_CUDA_TRY(cudaMemcpyAsync(pd, pair_offsets, (n_graphs + 1) * 8ULL, cudaMemcpyHostToDevice, st));
+  MCE_CUDA_TRY(cudaMemsetAsync(gmax, 0, (n_graphs + 1) * 4ULL, st));
+  const uint32_t gb = std::min<uint32_t>(n_graphs, 148 * 32);
+  k_graph_max_label<<<gb, 256, 0, st>>>(ud, vd, pd, n_graphs, gmax); note_launch();
+  k_plus_one<<<grid_for(n_graphs, 256), 256, 0, st>>>(gmax, n_graphs, pd); note_launch();
+  // label_base = exclusive prefix of (max label + 1); the total must fit in 31 bits
+  MCE_TRY(scan_exclusive_u32(gmax, base, n_graphs, base + n_graphs, st));
+  {
+    std::vector<uint32_t> gm(n_graphs);
+    MCE_CUDA_TRY(cudaMemcpyAsync(gm.data(), gmax, n_graphs * 4ULL, cudaMemcpyDeviceToHost, st));
+    MCE_CUDA_TRY(cudaStreamSynchronize(st));
+    uint64_t sum = 0;
+    for (uint32_t x : gm) sum += x;
+    if (sum >= (1ULL << 31)) return MCE_ERR_TOO_LARGE;
+  }
+  k_shift_pairs<<<gb, 256, 0, st>>>(ud, vd, pd, n_graphs, base); note_launch();
+  MCE_TRY(build_from_pairs(ud, vd, np, order, spin_limit, st, g));
+  unsigned int *nvd = nullptr, *mdd = nullptr, *dgd = nullptr;
+  unsigned long long *ned = nullptr;
+  if (cudaMallocAsync(&g->slot, std::max<uint32_t>(g->n, 1) * 4ULL, st) != cudaSuccess ||
+      cudaMallocAsync(&nvd, n_graphs * 4ULL, st) != cudaSuccess ||
+      cudaMallocAsync(&mdd, n_graphs * 4ULL, st) != cudaSuccess ||
+      cudaMallocAsync(&dgd, n_graphs * 4ULL, st) != cudaSuccess ||
+      cudaMallocAsync(&ned, n_graphs * 8ULL, st) != cudaSuccess)
+    return MCE_ERR_OUT_OF_MEMORY;
+  fr.p.push_back(nvd);
+  fr.p.push_back(mdd);
+  fr.p.push_back(dgd);
+  fr.p.push_back(ned);
+  cudaMemsetAsync(nvd, 0, n_graphs * 4ULL, st);
+  cudaMemsetAsync(mdd, 0, n_graphs * 4ULL, st);
+  cudaMemsetAsync(dgd, 0, n_graphs * 4ULL, st);
+  cudaMemsetAsync(ned, 0, n_graphs * 8ULL, st);
+  k_local_labels<<<grid_for(g->n, 256), 256, 0, st>>>(g->labels, g->h1, g->h2, g->slot, g->n, base, n_graphs);
+  note_launch();
+  k_count_per_graph<<<grid_for(std::max<uint64_t>(g->n, g->m), 256), 256, 0, st>>>(g->slot, g->n, g->root_v0, g->m,
+                                                                                  nvd, ned);
+  note_launch();
+  k_graph_degrees<<<grid_for(g->n, 256), 256, 0, st>>>(g->off, g->adj, g->n, g->slot, mdd, dgd);
+  note_launch();
+  counts->nv.resize(n_graphs);
+  counts->ne.resize(n_graphs);
+  counts->max_degree.resize(n_graphs);
+  counts->degeneracy.resize(n_graphs);
+  MCE_CUDA_TRY(cudaMemcpyAsync(counts->nv.data(), nvd, n_graphs * 4ULL, cudaMemcpyDeviceToHost, st));
+  MCE_CUDA_TRY(cudaMemcpyAsync(counts->ne.data(), ned, n_graphs * 8ULL, cudaMemcpyDeviceToHost, st));
+  MCE_CUDA_TRY(cudaMemcpyAsync(counts->max_degree.data(), mdd, n_graphs * 4ULL, cudaMemcpyDeviceToHost, st));
+  MCE_CUDA_TRY(cudaMemcpyAsync(counts->degeneracy.data(), dgd, n_graphs * 4ULL, cudaMemcpyDeviceToHost, st));
+  MCE_CUDA_TRY(cudaGetLastError());
+  MCE_CUDA_TRY(cudaStreamSynchronize(st));
+  return MCE_OK;
+}
+
 }  // namespace mce
 
 using namespace mce;
@@ -131,73 +221,25 @@ mce_status mce_batch_create(const uint32_t *u, const uint32_t *v, const uint64_t
   };
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(MCE_ERR_CUDA);
   cudaStream_t st = b->stream;
-  uint32_t *ud = nullptr, *vd = nullptr, *gmax = nullptr;
-  uint64_t *pd = nullptr;
+  uint32_t *ud = nullptr, *vd = nullptr;
   const size_t pb = std::max<uint64_t>(np, 1) * 4;
-  if (cudaMallocAsync(&ud, pb, st) != cudaSuccess || cudaMallocAsync(&vd, pb, st) != cudaSuccess ||
-      cudaMallocAsync(&pd, (n_graphs + 1) * 8ULL, st) != cudaSuccess ||
-      cudaMallocAsync(&gmax, (n_graphs + 1) * 4ULL, st) != cudaSuccess ||
-      cudaMallocAsync(&b->label_base, (n_graphs + 1) * 4ULL, st) != cudaSuccess)
+  if (cudaMallocAsync(&ud, pb, st) != cudaSuccess || cudaMallocAsync(&vd, pb, st) != cudaSuccess) {
+    if (ud) cudaFreeAsync(ud, st);
     return fail(MCE_ERR_OUT_OF_MEMORY);
+  }
   mce_status s = MCE_OK;
-  if ((np && (cudaMemcpyAsync(ud, u, np * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-              cudaMemcpyAsync(vd, v, np * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)) ||
-      cudaMemcpyAsync(pd, pair_offsets, (n_graphs + 1) * 8ULL, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-      cudaMemsetAsync(gmax, 0, (n_graphs + 1) * 4ULL, st) != cudaSuccess)
+  if (np && (cudaMemcpyAsync(ud, u, np * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+             cudaMemcpyAsync(vd, v, np * 4, cudaMemcpyHostToDevice, st) != cudaSuccess))
     s = MCE_ERR_CUDA;
-  if (s == MCE_OK) {
-    const uint32_t gb = std::min<uint32_t>(n_graphs, 148 * 32);
-    k_graph_max_label<<<gb, 256, 0, st>>>(ud, vd, pd, n_graphs, gmax); note_launch();
-    k_plus_one<<<grid_for(n_graphs, 256), 256, 0, st>>>(gmax, n_graphs, pd); note_launch();
-    // label_base = exclusive prefix of (max label + 1); the total must fit in 32 bits
-    s = scan_exclusive_u32(gmax, b->label_base, n_graphs, b->label_base + n_graphs, st);
-  }
-  if (s == MCE_OK) {
-    // overflow check: recompute the sum in 64 bits on the host
-    std::vector<uint32_t> gm(n_graphs);
-    if (cudaMemcpyAsync(gm.data(), gmax, n_graphs * 4ULL, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-      s = MCE_ERR_CUDA;
-    uint64_t sum = 0;
-    for (uint32_t x : gm) sum += x;
-    if (s == MCE_OK && sum >= (1ULL << 31)) s = MCE_ERR_TOO_LARGE;
-  }
-  if (s == MCE_OK) {
-    const uint32_t gb = std::min<uint32_t>(n_graphs, 148 * 32);
-    k_shift_pairs<<<gb, 256, 0, st>>>(ud, vd, pd, n_graphs, b->label_base); note_launch();
-    s = build_from_pairs(ud, vd, np, o.order, o.spin_limit ? o.spin_limit : (1ULL << 34), st, &b->g);
-  }
+  UnionCounts uc;
+  if (s == MCE_OK)
+    s = build_union(ud, vd, pair_offsets, n_graphs, o.order, o.spin_limit ? o.spin_limit : (1ULL << 34), st, &b->g,
+                    &uc);
   cudaFreeAsync(ud, st);
   cudaFreeAsync(vd, st);
-  cudaFreeAsync(gmax, st);
-  if (s != MCE_OK) {
-    cudaFreeAsync(pd, st);
-    return fail(s);
-  }
-  unsigned int *nvd = nullptr;
-  unsigned long long *ned = nullptr;
-  if (cudaMallocAsync(&b->g.slot, std::max<uint32_t>(b->g.n, 1) * 4ULL, st) != cudaSuccess ||
-      cudaMallocAsync(&nvd, n_graphs * 4ULL, st) != cudaSuccess ||
-      cudaMallocAsync(&ned, n_graphs * 8ULL, st) != cudaSuccess) {
-    cudaFreeAsync(pd, st);
-    return fail(MCE_ERR_OUT_OF_MEMORY);
-  }
-  cudaMemsetAsync(nvd, 0, n_graphs * 4ULL, st);
-  cudaMemsetAsync(ned, 0, n_graphs * 8ULL, st);
-  k_local_labels<<<grid_for(b->g.n, 256), 256, 0, st>>>(b->g.labels, b->g.h1, b->g.h2, b->g.slot, b->g.n,
-                                                          b->label_base, n_graphs); note_launch();
-  k_count_per_graph<<<grid_for(std::max<uint64_t>(b->g.n, b->g.m), 256), 256, 0, st>>>(b->g.slot, b->g.n,
-                                                                                      b->g.root_v0, b->g.m, nvd, ned); note_launch();
-  b->nv.resize(n_graphs);
-  b->ne.resize(n_graphs);
-  if (cudaMemcpyAsync(b->nv.data(), nvd, n_graphs * 4ULL, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-      cudaMemcpyAsync(b->ne.data(), ned, n_graphs * 8ULL, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-      cudaStreamSynchronize(st) != cudaSuccess)
-    s = MCE_ERR_CUDA;
-  cudaFreeAsync(nvd, st);
-  cudaFreeAsync(ned, st);
-  cudaFreeAsync(pd, st);
   if (s != MCE_OK) return fail(s);
+  b->nv = std::move(uc.nv);
+  b->ne = std::move(uc.ne);
   *out = b;
   return MCE_OK;
 }
@@ -302,7 +344,6 @@ void mce_batch_free(mce_batch *b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->stream) cudaStreamSynchronize(b->stream);
   free_graph(&b->g);
-  if (b->label_base) cudaFree(b->label_base);
   if (b->slots_h) cudaFreeHost(b->slots_h);
   if (b->hist_h) cudaFreeHost(b->hist_h);
   b->scr.release();

@@ -119,6 +119,10 @@ mce_status reduce_max_u32(const uint32_t *in, uint64_t n, uint32_t *d_out, cudaS
 struct Scratch {
   static constexpr int kSlots = 8;
   int device = 0;
+  // set: buffers are allocated and freed stream-ordered on this stream (no
+  // device-wide synchronisation when one grows), for an owner whose work
+  // stays on that stream (a server dispatcher)
+  cudaStream_t ordered = nullptr;
   void *ptr[kSlots] = {};
   size_t bytes[kSlots] = {};
   void *get(int purpose, size_t n, mce_status *st);

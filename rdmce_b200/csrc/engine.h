@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <vector>
 
 #include "common.cuh"
 #include "internal.h"
@@ -38,6 +39,20 @@ mce_status build_from_csr(uint64_t n, const uint32_t *off_d, const uint32_t *adj
 mce_status csr_to_edges(uint64_t n, const uint32_t *off, const uint32_t *adj, uint64_t m, uint32_t *deg,
                         uint32_t **eu, uint32_t **ev, cudaStream_t st);
 void free_graph(DeviceGraph *g);
+// Per-graph figures of a union build (build_union).
+struct UnionCounts {
+  std::vector<uint32_t> nv;          // vertices
+  std::vector<uint64_t> ne;          // undirected edges
+  std::vector<uint32_t> max_degree;
+  std::vector<uint32_t> degeneracy;
+};
+// Disjoint union of graphs whose COO pairs are in device memory, graph i
+// being pairs [pair_offsets[i], pair_offsets[i + 1]) (host offsets): labels
+// are shifted into disjoint ranges (ud, vd are modified), the union is built
+// as one graph, and every vertex gets its graph as result slot and its own
+// label back (batch.cu).
+mce_status build_union(uint32_t *ud, uint32_t *vd, const uint64_t *pair_offsets, uint32_t n_graphs, int order,
+                       uint64_t spin_limit, cudaStream_t st, DeviceGraph *g, UnionCounts *counts);
 // first use of a device in this process: its default stream-ordered memory
 // pool keeps freed memory for reuse instead of returning it at every sync
 void keep_pool_memory(int device);

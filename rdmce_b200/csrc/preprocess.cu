@@ -322,15 +322,13 @@ mce_status peel(uint32_t n, const uint32_t *off, const uint32_t *adj, const uint
   MCE_CUDA_TRY(cudaMemcpyAsync(deg.p, deg0, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
   MCE_CUDA_TRY(cudaMemsetAsync(state.p, 0, n * sizeof(uint32_t), st));
   k_iota<<<grid_for(n, 256), 256, 0, st>>>(remA.p, n); note_launch();
+  // the control block goes through ordinary host memory: pinning it for each
+  // build (and unpinning, which synchronises the device) would stall other
+  // streams' work, e.g. concurrently served requests
   PeelCtl h{};
   for (int i = 0; i < 3; i++) h.rmin[i] = 0xffffffffu;
-  PeelCtl *hc = nullptr;
-  MCE_CUDA_TRY(cudaMallocHost(&hc, sizeof(PeelCtl)));
-  struct FreeHost {
-    void *p;
-    ~FreeHost() { cudaFreeHost(p); }
-  } free_hc{hc};
-  *hc = h;
+  PeelCtl hc_buf = h;
+  PeelCtl *hc = &hc_buf;
   MCE_CUDA_TRY(cudaMemcpyAsync(ctl.p, hc, sizeof(PeelCtl), cudaMemcpyHostToDevice, st));
   int dev = 0, sms = 0, per_sm = 0;
   MCE_CUDA_TRY(cudaGetDevice(&dev));

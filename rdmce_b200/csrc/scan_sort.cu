@@ -338,10 +338,15 @@ void *Scratch::get(int purpose, size_t n, mce_status *st) {
     return nullptr;
   }
   if (ptr[purpose] && bytes[purpose] >= n) return ptr[purpose];
-  if (ptr[purpose]) cudaFree(ptr[purpose]);
+  if (ptr[purpose]) {
+    if (ordered) cudaFreeAsync(ptr[purpose], ordered);
+    else cudaFree(ptr[purpose]);
+  }
   ptr[purpose] = nullptr;
   bytes[purpose] = 0;
-  if (cudaMalloc(&ptr[purpose], std::max<size_t>(n, 256)) != cudaSuccess) {
+  const cudaError_t e = ordered ? cudaMallocAsync(&ptr[purpose], std::max<size_t>(n, 256), ordered)
+                                : cudaMalloc(&ptr[purpose], std::max<size_t>(n, 256));
+  if (e != cudaSuccess) {
     cudaGetLastError();
     ptr[purpose] = nullptr;
     *st = MCE_ERR_OUT_OF_MEMORY;
@@ -352,11 +357,17 @@ void *Scratch::get(int purpose, size_t n, mce_status *st) {
 }
 
 void Scratch::release() {
+  bool freed = false;
   for (int i = 0; i < kSlots; i++) {
-    if (ptr[i]) cudaFree(ptr[i]);
+    if (ptr[i]) {
+      if (ordered) cudaFreeAsync(ptr[i], ordered);
+      else cudaFree(ptr[i]);
+      freed = true;
+    }
     ptr[i] = nullptr;
     bytes[i] = 0;
   }
+  if (ordered && freed) cudaStreamSynchronize(ordered);
 }
 
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }

@@ -79,6 +79,8 @@ def test_server_results_alone_and_in_the_mix(gpu):
         r, lat = g
         assert lat > 0
         assert (r.count, r.checksum, r.hist) == (a.count, a.checksum, a.hist), k
+        assert (r.num_vertices, r.num_edges, r.degeneracy, r.max_degree) == (a.num_vertices, a.num_edges,
+                                                                              a.degeneracy, a.max_degree), k
     # the mix really shared the device: sweep the requests' device-clock spans
     assert max_overlap(spans) >= 2, spans
 
