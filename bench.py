@@ -61,6 +61,21 @@ FIXTURE24 = os.path.join(ROOT, "tests", "golden", "samples", "rmat24_sample.json
 LIGHT_ROOT = 10_000_000
 
 
+def profiled_traffic(workload):
+    """DRAM bytes (read + write) of one k_enumerate launch of this workload,
+    as the committed ncu summary records them; None where none was taken."""
+    if workload != "rmat20-sample":
+        return None
+    try:
+        with open(os.path.join(ROOT, "profiles", "k_enumerate_dram_traffic.md")) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch_rmat20_sample:"):
+                    return int(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def load_fixture():
     with open(FIXTURE) as f:
         return json.load(f)
@@ -511,10 +526,15 @@ def run_ours(args):
             "config": config,
             "parity": parity,
             "roofline": {"bound": "int", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gword-ops/s",
-                         "frac": achieved / peak if peak else None, "traffic": None,
+                         "frac": achieved / peak if peak else None,
+                         "traffic": profiled_traffic(args.workload),
+                         "build_bytes": int(rs.build_bytes),
                          "note": "bitmap row word-ops of one step (ANDN+POPC per active row per node, row "
                                  "filters; counted by an untimed MCE_FLAG_STATS solve of the same sample) / the "
-                                 "timed k_enumerate time per step; peak = live INT-pipe probe of the same op mix"},
+                                 "timed k_enumerate time per step; peak = live INT-pipe probe of the same op mix; "
+                                 "traffic = DRAM read+write bytes of one k_enumerate launch of this workload from "
+                                 "ncu (profiles/k_enumerate_dram_traffic.md); build_bytes = the algorithmic "
+                                 "ego-network build bytes of one step, counted by the same untimed solve"},
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": int(u.nbytes + v.nbytes + (0 if full and world == 1 else roots.nbytes)),
                     "d2h_bytes_per_step": int(C.sizeof(mce._Result)),
