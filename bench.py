@@ -433,9 +433,11 @@ def run_ours(args):
     cycles = [0] * 6
     cliques = 0
     used = set()
+    longest = []  # per step: the longest root and the longest task, in warp clock cycles
     for _ in range(args.steps):
         r, ms = step()
         used.add((r.blocks_per_sm, r.autotune))
+        longest.append([int(x) for x in r.max_item_cycles])
         if ref is not None and (r.count, r.checksum) != ref:
             raise RuntimeError(f"nondeterministic result: {(r.count, r.checksum)} vs {ref}")
         ref = (r.count, r.checksum)
@@ -550,6 +552,8 @@ def run_ours(args):
             "search": {"nodes_per_step": int(nodes), "word_ops_per_step": int(wops),
                        "nodes_per_s": nodes / (enum_ms_step / 1000.0) if enum_ms_step else None,
                        "enumerate_ms_per_step": enum_ms / args.steps,
+                       "step_ms": [round(t, 3) for t in times],
+                       "longest_item_cycles": longest,
                        "enum_launches_per_step": launches_enum / args.steps,
                        "warp_cycle_share": {k: round(c / max(1, sum(cycles)), 4) for k, c in
                                             zip(["build", "register", "general", "spawn", "idle", "queue"],

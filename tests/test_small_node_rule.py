@@ -47,3 +47,82 @@ def test_rule_reproduces_maximal_cliques(seed):
     order = sorted(g, key=lambda v: (nx.core_number(g)[v], v))
     want = {frozenset(c) for c in nx.find_cliques(g)}
     assert cliques_by_rule(g, order) == want
+
+
+def lanes_with_bit(k):
+    """Lanes (subsets 0..31) whose index has bit k set, as a 32-bit mask."""
+    return sum(1 << s for s in range(32) if (s >> k) & 1)
+
+
+def decide_by_masks(n, adj, holds):
+    """The 32-bit tier's one-step decision of a node with n (3..7) candidates,
+    restated with its warp-uniform masks: subset s = 32 g + lane, the lane
+    index carrying candidates 0..4 and the group g the rest.  adj[i] is the
+    candidate-adjacency bitmask of candidate i; holds[k] is the set of active
+    rows containing candidate k (as a bitmask over rows).  Returns the subsets
+    the kernel emits."""
+    nl = min(n, 5)
+    ng = n - nl
+    notclique = 0
+    for i, j in itertools.combinations(range(nl), 2):
+        if not (adj[i] >> j) & 1:
+            notclique |= lanes_with_bit(i) & lanes_with_bit(j)
+    full = (1 << 64) - 1
+    out = set()
+    for g in range(1 << ng):
+        group_clique = True
+        far_all = 0
+        for b in range(ng):
+            if not (g >> b) & 1:
+                continue
+            u = nl + b
+            for i in range(nl):
+                if not (adj[i] >> u) & 1:
+                    far_all |= lanes_with_bit(i)
+            for b2 in range(b + 1, ng):
+                if (g >> b2) & 1 and not (adj[u] >> (nl + b2)) & 1:
+                    group_clique = False
+        for lane in range(32):
+            if lane >= (1 << nl) or (notclique >> lane) & 1 or (g == 0 and lane == 0):
+                continue
+            if (far_all >> lane) & 1 or not group_clique:
+                continue
+            rows = full
+            members = [k for k in range(nl) if (lane >> k) & 1] + [nl + b for b in range(ng) if (g >> b) & 1]
+            for k in members:
+                rows &= holds[k]
+            if rows == 0:
+                out.add(sum(1 << k for k in members))
+    return out
+
+
+def decide_directly(n, adj, holds):
+    out = set()
+    for s in range(1, 1 << n):
+        members = [k for k in range(n) if (s >> k) & 1]
+        if any(not (adj[i] >> j) & 1 for i, j in itertools.combinations(members, 2)):
+            continue
+        rows = (1 << 64) - 1
+        for k in members:
+            rows &= holds[k]
+        if rows == 0:
+            out.add(s)
+    return out
+
+
+@pytest.mark.parametrize("n", [3, 4, 5, 6, 7])
+def test_subset_masks_match_direct_decision(n):
+    """The kernel's lane and group masks select exactly the cliques of the
+    candidates that no active row contains, for 3 to 7 candidates."""
+    rnd = random.Random(100 + n)
+    for _ in range(300):
+        p = rnd.choice([0.3, 0.6, 0.85, 1.0])
+        adj = [0] * n
+        for i, j in itertools.combinations(range(n), 2):
+            if rnd.random() < p:
+                adj[i] |= 1 << j
+                adj[j] |= 1 << i
+        nrows = rnd.randint(0, 12)
+        rows = [sum(1 << k for k in range(n) if rnd.random() < 0.5) for _ in range(nrows)]
+        holds = [sum(1 << r for r, row in enumerate(rows) if (row >> k) & 1) for k in range(n)]
+        assert decide_by_masks(n, adj, holds) == decide_directly(n, adj, holds)
