@@ -110,8 +110,9 @@ typedef struct mce_result {
                                  per root 4 (d(v0) + d(v1)) + sum over members u of P and X of
                                  (4 d(u) + 8 W), W = ceil(|P| / 64) */
   uint64_t launches;          /* enumeration kernel launches */
-  uint64_t warp_cycles[6];    /* warp clock cycles by phase: root build, register tiers,
-                                 general tier, exposing tasks, idle, queue */
+  uint64_t warp_cycles[8];    /* warp clock cycles by phase: [0] root build, [1] 64-bit tier,
+                                 [2] general tier, [3] exposing tasks, [4] idle, [5] queue,
+                                 [6] 32-bit tier, [7] reserved (0) */
   uint64_t max_item_cycles[2]; /* longest single work item, in warp clock cycles: [0] a root,
                                   [1] a task taken from another warp */
   double phase_ms[MCE_PHASES];

@@ -79,7 +79,7 @@ class _Result(C.Structure):
         ("word_ops", C.c_uint64),
         ("build_bytes", C.c_uint64),
         ("launches", C.c_uint64),
-        ("warp_cycles", C.c_uint64 * 6),
+        ("warp_cycles", C.c_uint64 * 8),
         ("max_item_cycles", C.c_uint64 * 2),
         ("phase_ms", C.c_double * PHASES),
         ("hist", C.c_uint64 * HIST_LEN),

@@ -473,7 +473,7 @@ static mce_status solve_impl(mce_graph *g, const mce_options &o, mce_result *out
   out->word_ops = stats.word_ops;
   out->build_bytes = stats.build_bytes;
   out->launches = stats.launches;
-  for (int i = 0; i < 6; i++) out->warp_cycles[i] = stats.cycles[i];
+  for (int i = 0; i < 8; i++) out->warp_cycles[i] = stats.cycles[i];
   for (int i = 0; i < 2; i++) out->max_item_cycles[i] = stats.max_item[i];
   out->status_detail = stats.error;
   out->phase_ms[MCE_PHASE_H2D] = g->ms_h2d;

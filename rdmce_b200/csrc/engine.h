@@ -116,10 +116,11 @@ struct EnumStats {
   uint64_t heavy_roots = 0;
   uint64_t shared_tasks = 0;
   uint64_t nodes = 0, word_ops = 0, build_bytes = 0;
-  uint64_t cycles[6] = {0, 0, 0, 0, 0, 0};
+  uint64_t cycles[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   uint64_t max_item[2] = {0, 0};  // longest root, longest task (cycles)
   uint32_t error = 0;
   float ms_setup = 0, ms_enum = 0;
+  float ms_heavy = 0;  // device time of the deferred-root pass (part of ms_enum)
   uint64_t launches = 0;
   uint32_t blocks_per_sm = 0;  // resident 8-warp blocks per SM the solve ran with
 };
@@ -168,7 +169,7 @@ struct EnumParams {
   unsigned long long *stat_nodes;
   unsigned long long *stat_wops;
   unsigned long long *stat_bbytes;       // algorithmic ego-network build bytes (stats mode)
-  unsigned long long *stat_cycles;       // per phase: build, register tiers, general tier, spawn, idle, queue
+  unsigned long long *stat_cycles;       // per phase: build, 64-bit tier, general tier, spawn, idle, queue, 32-bit tier
   unsigned long long *stat_max_item;     // [2]: longest root, longest task, in cycles
   unsigned int *active;                  // warps holding work
   // task pool: blocks of block_bytes, a free ring and a ready ring (one cell per block)

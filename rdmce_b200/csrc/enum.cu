@@ -78,9 +78,15 @@ constexpr uint32_t kLocalRec = 2048;      // per-warp local task record (64-bit-
 // with fewer, larger tasks, once nested tiers expose their outer levels first.
 constexpr uint32_t kRegShareBound = 24;
 constexpr uint32_t kShareMin = 128, kShareMax = 8192;
-constexpr int kSmallP = 5;  // 32-bit-tier nodes with this few candidates are decided in one step
+// 32-bit-tier nodes with this few candidates (5, 6 or 7) are decided in one step
+#ifndef MCE_SMALL_P
+#define MCE_SMALL_P 6
+#endif
+constexpr int kSmallP = MCE_SMALL_P;
+static_assert(kSmallP >= 5 && kSmallP <= 7, "small-node decisions cover up to 5, 6 or 7 candidates");
 // phases of the per-warp cycle accounting
-enum { kCycBuild = 0, kCycReg = 1, kCycGen = 2, kCycSpawn = 3, kCycIdle = 4, kCycQueue = 5, kCycPhases = 6 };
+// (kCycReg: the 64-bit tier; kCycT0: the 32-bit tier)
+enum { kCycBuild = 0, kCycReg = 1, kCycGen = 2, kCycSpawn = 3, kCycIdle = 4, kCycQueue = 5, kCycT0 = 6, kCycPhases = 7 };
 
 struct TaskHdr {
   uint32_t pc;     // candidate columns
@@ -558,15 +564,22 @@ __device__ __forceinline__ constexpr uint32_t lanes_with_bit(int k) {
   return k == 0 ? 0xAAAAAAAAu : k == 1 ? 0xCCCCCCCCu : k == 2 ? 0xF0F0F0F0u : k == 3 ? 0xFF00FF00u : 0xFFFF0000u;
 }
 
-// A node with exactly N (3..5) candidates, decided in one step.  R + K is a
+// A node with exactly N (3..7) candidates, decided in one step.  R + K is a
 // maximal clique for exactly the cliques K of the candidates that no active
-// row contains (a candidate outside K that extends K is itself such a row);
-// lane s tests the subset s.  Whether s is a clique is read off a warp-uniform
-// mask: each missing edge (i, j) excludes the lanes with bits i and j.  Rows
-// containing s: the AND of the per-candidate ballots over s's members.
+// row contains (a candidate outside K that extends K is itself such a row).
+// The subsets are numbered s = 32 g + lane: the lane index carries the
+// subset's lowest five candidates, the group g (one pass each, 2^(N-5) of
+// them) the rest.  Whether s is a clique is read off warp-uniform masks: a
+// missing edge (i, j) among the lane's candidates excludes the lanes with bits
+// i and j; a missing edge from a group candidate u to candidate i excludes the
+// lanes with bit i in the groups holding u; a missing edge between two group
+// candidates excludes whole groups.  Rows containing s: the AND of the
+// per-candidate ballots over s's members.
 template <int N>
 __device__ __forceinline__ void t0_small_n(const Ctx &c, const T0 &t, uint32_t P, uint32_t A, uint32_t RM,
                                            uint32_t &npend, uint64_t s10, uint64_t s20, uint32_t rsize0) {
+  constexpr int NL = N < 5 ? N : 5;  // candidates carried by the lane index
+  constexpr int NG = N - NL;         // candidates carried by the group
   WarpSmem *sm = c.sm;
   const uint32_t lane = c.lane;
   uint32_t qb[N], h[N], r[N - 1];
@@ -583,26 +596,48 @@ __device__ __forceinline__ void t0_small_n(const Ctx &c, const T0 &t, uint32_t P
   for (int k = 0; k < N - 1; k++) r[k] = __shfl_sync(kFull, t.row, __ffs(qb[k]) - 1);
   uint32_t notclique = 0;
 #pragma unroll
-  for (int i = 0; i < N - 1; i++)
+  for (int i = 0; i < NL - 1; i++)
 #pragma unroll
-    for (int j = i + 1; j < N; j++)
+    for (int j = i + 1; j < NL; j++)
       if (!(r[i] & qb[j])) notclique |= lanes_with_bit(i) & lanes_with_bit(j);
   uint32_t rows = A, mask = RM;
 #pragma unroll
-  for (int k = 0; k < N; k++)
+  for (int k = 0; k < NL; k++)
     if ((lane >> k) & 1) {
       rows &= h[k];
       mask |= qb[k];
     }
-  const bool out = lane != 0 && lane < (1u << N) && !((notclique >> lane) & 1) && rows == 0;
-  const uint32_t E = __ballot_sync(kFull, out);
-  const uint32_t pos = npend + __popc(E & lanemask_lt());
-  if (out && pos < 32) sm->pend_rm[pos] = mask;
-  npend += __popc(E);
-  if (npend >= 32) {
-    t0_flush(c, 32, s10, s20, rsize0);
-    if (out && pos >= 32) sm->pend_rm[pos - 32] = mask;
-    npend -= 32;
+  const bool lane_ok = lane < (1u << NL) && !((notclique >> lane) & 1);
+#pragma unroll
+  for (int g = 0; g < (1 << NG); g++) {
+    bool ok = lane_ok && (g != 0 || lane != 0);
+    bool group_clique = true;
+    uint32_t rg = rows, mg = mask;
+#pragma unroll
+    for (int b = 0; b < NG; b++) {
+      if (!((g >> b) & 1)) continue;
+      const int u = NL + b;
+      uint32_t far = 0;  // lanes holding a candidate not adjacent to u
+#pragma unroll
+      for (int i = 0; i < NL; i++)
+        if (!(r[i] & qb[u])) far |= lanes_with_bit(i);
+      ok = ok && !((far >> lane) & 1);
+      rg &= h[u];
+      mg |= qb[u];
+#pragma unroll
+      for (int b2 = b + 1; b2 < NG; b2++)
+        if (((g >> b2) & 1) && !(r[u] & qb[NL + b2])) group_clique = false;
+    }
+    const bool out = group_clique && ok && rg == 0;
+    const uint32_t E = __ballot_sync(kFull, out);
+    const uint32_t pos = npend + __popc(E & lanemask_lt());
+    if (out && pos < 32) sm->pend_rm[pos] = mg;
+    npend += __popc(E);
+    if (npend >= 32) {
+      t0_flush(c, 32, s10, s20, rsize0);
+      if (out && pos >= 32) sm->pend_rm[pos - 32] = mg;
+      npend -= 32;
+    }
   }
 }
 
@@ -655,7 +690,13 @@ __device__ __forceinline__ void t0_small(const Ctx &c, const T0 &t, uint32_t P, 
   switch (__popc(P)) {
     case 3: t0_small_n<3>(c, t, P, A, RM, npend, s10, s20, rsize0); break;
     case 4: t0_small_n<4>(c, t, P, A, RM, npend, s10, s20, rsize0); break;
-    default: t0_small_n<5>(c, t, P, A, RM, npend, s10, s20, rsize0); break;
+#if MCE_SMALL_P >= 6
+    case 5: t0_small_n<5>(c, t, P, A, RM, npend, s10, s20, rsize0); break;
+#endif
+#if MCE_SMALL_P >= 7
+    case 6: t0_small_n<6>(c, t, P, A, RM, npend, s10, s20, rsize0); break;
+#endif
+    default: t0_small_n<kSmallP < 3 ? 3 : kSmallP>(c, t, P, A, RM, npend, s10, s20, rsize0); break;
   }
 }
 
@@ -831,7 +872,7 @@ __device__ __forceinline__ void t0_solve(const Ctx &c, const T0 &t, uint32_t pc,
                                          uint64_t s10, uint64_t s20) {
   const unsigned long long t0 = now(), sp0 = c.sm->cyc[kCycSpawn];
   t0_run(c, t, pc, nrows, rsize0, s10, s20);
-  if (c.lane == 0) c.sm->cyc[kCycReg] += (now() - t0) - (c.sm->cyc[kCycSpawn] - sp0);
+  if (c.lane == 0) c.sm->cyc[kCycT0] += (now() - t0) - (c.sm->cyc[kCycSpawn] - sp0);
 }
 
 // a W = 1 record with pc <= 32 and nrows <= 32, from a pool block (cg loads)
@@ -1108,7 +1149,15 @@ __device__ __noinline__ void t1_solve_body(Ctx c, T1 t, uint32_t pc, uint32_t nr
         t0.h2 = lane < pc2 ? sm->xh2[lane] : 0;
         if (lane == 0) sm->t1_level = level;
         __syncwarp();
+        const unsigned long long tn = now(), spn = sm->cyc[kCycSpawn];
         t0_run(c, t0, pc2, nact, rs, n1, n2);
+        if (lane == 0) {
+          // the child's cycles go to the 32-bit tier (t1_solve adds the whole
+          // span to the 64-bit tier afterwards)
+          const unsigned long long dt = (now() - tn) - (sm->cyc[kCycSpawn] - spn);
+          sm->cyc[kCycT0] += dt;
+          sm->cyc[kCycReg] -= dt;
+        }
         // the child may have exposed open candidates of this level
         VP = ta->fVP[level];
         // While the child ran, the levels above it were exposed only through
@@ -2337,14 +2386,28 @@ mce_status MCE_ENUM_FN(enum_finish)(const EnumPlan &plan, cudaStream_t st, EnumS
     H.params.n_heavy = h.heavy_n;
     H.params.push_heavy = 0;
     H.params.nwarps = (uint32_t)H.nwarps;
-    MCE_TRY(reset_ctl(H, st));
-    k_enumerate<<<H.blocks, H.threads, H.smem, st>>>(H.params);
-    note_launch();
-    launches++;
-    MCE_CUDA_TRY(cudaGetLastError());
+    cudaEvent_t he0, he1;
+    MCE_CUDA_TRY(cudaEventCreate(&he0));
+    MCE_CUDA_TRY(cudaEventCreate(&he1));
+    cudaEventRecord(he0, st);
+    mce_status ls = reset_ctl(H, st);
+    if (ls == MCE_OK) {
+      k_enumerate<<<H.blocks, H.threads, H.smem, st>>>(H.params);
+      note_launch();
+      launches++;
+      if (cudaGetLastError() != cudaSuccess) ls = MCE_ERR_CUDA;
+    }
+    cudaEventRecord(he1, st);
     EnumCtl h2{};
-    MCE_CUDA_TRY(cudaMemcpyAsync(&h2, ctl, sizeof(EnumCtl), cudaMemcpyDeviceToHost, st));
-    MCE_CUDA_TRY(cudaStreamSynchronize(st));
+    if (ls == MCE_OK && cudaMemcpyAsync(&h2, ctl, sizeof(EnumCtl), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      ls = MCE_ERR_CUDA;
+    if (ls == MCE_OK && cudaStreamSynchronize(st) != cudaSuccess) ls = MCE_ERR_CUDA;
+    float hms = 0;
+    if (ls == MCE_OK) cudaEventElapsedTime(&hms, he0, he1);
+    cudaEventDestroy(he0);
+    cudaEventDestroy(he1);
+    if (ls != MCE_OK) return ls;
+    if (stats) stats->ms_heavy = hms;
     roots = roots - heavy_roots + h2.stat_roots;
     tasks += h2.stat_tasks;
     nodes += h2.stat_nodes;

@@ -68,17 +68,21 @@ mce_status enumerate(const DeviceGraph &g, const EnumConfig &cfg, Scratch *scr, 
   cudaEvent_t e0, e1;
   MCE_CUDA_TRY(cudaEventCreate(&e0));
   MCE_CUDA_TRY(cudaEventCreate(&e1));
+  // device time of the launch alone: e1 is recorded right behind the kernel,
+  // before the host reads the control block back (a host that is slow to
+  // wake from that wait adds nothing); a deferred-root pass adds its own
   cudaEventRecord(e0, st);
   mce_status s = enum_launch(plan, st);
-  if (s == MCE_OK) s = enum_finish(plan, st, stats);
   cudaEventRecord(e1, st);
+  EnumStats local;
+  if (s == MCE_OK) s = enum_finish(plan, st, stats ? stats : &local);
   cudaEventSynchronize(e1);
   float ms = 0;
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (stats) {
-    stats->ms_enum = ms;
+    stats->ms_enum = ms + stats->ms_heavy;
     stats->blocks_per_sm = plan.blocks / std::max<uint32_t>(1, plan.sms);
   }
   return s;
