@@ -78,9 +78,12 @@ constexpr uint32_t kLocalRec = 2048;      // per-warp local task record (64-bit-
 // with fewer, larger tasks, once nested tiers expose their outer levels first.
 constexpr uint32_t kRegShareBound = 24;
 constexpr uint32_t kShareMin = 128, kShareMax = 8192;
-// 32-bit-tier nodes with this few candidates (5, 6 or 7) are decided in one step
+// 32-bit-tier nodes with this few candidates (5, 6 or 7) are decided in one
+// step.  Larger limits take more nodes off the search tree but grow the node
+// loop's code, and with the join decision below taking the large nodes, the
+// instruction cache is the tighter bound: 5 measured fastest.
 #ifndef MCE_SMALL_P
-#define MCE_SMALL_P 6
+#define MCE_SMALL_P 5
 #endif
 constexpr int kSmallP = MCE_SMALL_P;
 static_assert(kSmallP >= 5 && kSmallP <= 7, "small-node decisions cover up to 5, 6 or 7 candidates");
@@ -449,7 +452,9 @@ struct T0 {
 
 // Hash the pending leaves, one per lane: sums of the entry sums and the R
 // columns' hashes, then the clique hash, histogram and largest size.
-__device__ __forceinline__ void t0_flush(const Ctx &c, uint32_t npend, uint64_t s10, uint64_t s20,
+// Out of line: it runs once per 32 leaves, and one copy keeps the hot node
+// loop's code small (instruction-cache misses, not issue slots, bound it).
+__device__ __noinline__ void t0_flush(Ctx c, uint32_t npend, uint64_t s10, uint64_t s20,
                                          uint32_t rsize0) {
   WarpSmem *sm = c.sm;
   const uint32_t lane = c.lane;
@@ -700,6 +705,212 @@ __device__ __forceinline__ void t0_small(const Ctx &c, const T0 &t, uint32_t P, 
   }
 }
 
+// ------------------------------------------------ join decomposition
+// A node whose active rows are all candidates (no X row contains R) has as
+// its maximal cliques R + K for exactly the maximal cliques K of G[P].  Let H
+// be the complement of G[P].  G[P] is the join of the complements of H's
+// connected components, so its maximal cliques are the products of one
+// maximal clique of each component's complement, i.e. one maximal independent
+// set (in H) per component.  When every component is small, the node is
+// decided without a search tree: count, histogram and largest size in closed
+// form, and the checksum by walking the products, 32 lanes at a time.
+//
+// Components: breadth-first search with ballots (closed H-neighbourhoods
+// nb = P \ row).  Component j's maximal independent sets come from the 2^s
+// subsets of its s members, one per lane, and are packed into a table of at
+// most 32 entries in shared memory (hash sums and size of each set).  Lane j
+// holds component j's first entry and entry count.
+//
+// Walking the products: the first components whose entry counts multiply to
+// at most 32 (Q) are carried by the lane index (each lane adds up its own
+// entries once); the others form a warp-uniform mixed-radix counter, whose
+// steps swap one entry per digit that moves.
+constexpr int kJoinComp = 5;    // largest component decided this way
+#ifndef MCE_JOIN_MIN
+#define MCE_JOIN_MIN 10
+#endif
+constexpr int kJoinMin = MCE_JOIN_MIN;  // smallest |P| worth the decomposition
+
+__device__ __noinline__ bool t0_join(Ctx c, T0 t, uint32_t P, uint32_t RM, uint64_t s10, uint64_t s20,
+                                     uint32_t rsize0) {
+  const uint32_t lane = c.lane;
+  WarpSmem *sm = c.sm;
+  const bool inP = (P >> lane) & 1;
+  const uint32_t nb = inP ? (P & ~t.row) : 0u;  // closed non-neighbourhood in P (rows carry no self bit)
+  if (__reduce_max_sync(kFull, (uint32_t)__popc(nb)) > (uint32_t)kJoinComp) return false;
+  const uint32_t single = __ballot_sync(kFull, inP && nb == (1u << lane));  // adjacent to every candidate
+  // components first: a node is abandoned before any set is built
+  uint32_t rem = P & ~single;
+  uint32_t comp = 0, ncomp = 0;  // lane j: component j's members
+  #pragma unroll 1
+  while (rem) {
+    uint32_t C = rem & (0u - rem), fr = C;
+    do {
+      const uint32_t nbr = __ballot_sync(kFull, (nb & fr) != 0);
+      fr = nbr & ~C;
+      C |= nbr;
+    } while (fr && __popc(C) <= kJoinComp);
+    if (__popc(C) > kJoinComp) return false;
+    if (lane == ncomp) comp = C;
+    ncomp++;
+    rem &= ~C;
+  }
+  // Scratch while the node is decided: the exchange buffer and the row buffer
+  // (free inside a 32-bit-tier solve).  xrow: closed non-neighbourhoods by
+  // column; rowbuf[e], rowbuf[32 + e], xcv[e]: entry e's hash sums and size.
+  uint64_t *E1 = sm->rowbuf, *E2 = sm->rowbuf + 32;
+  uint32_t *ES = sm->xcv;
+  sm->xrow[lane] = nb;
+  __syncwarp();
+  uint32_t nent = 0, c_off = 0, c_r = 0;  // lane j: component j's first entry and entry count
+  uint64_t total = 1;
+  #pragma unroll 1
+  for (uint32_t j = 0; j < ncomp; j++) {
+    const uint32_t C = __shfl_sync(kFull, comp, j);
+    const uint32_t ns = __popc(C);
+    // lane l tests the subset l of C's members (bit k = k-th lowest member)
+    uint32_t sub = 0;
+    uint64_t a1 = 0, a2 = 0;
+    uint32_t cm = C;
+    #pragma unroll 1
+    for (uint32_t k = 0; k < ns; k++) {
+      const uint32_t b = cm & (0u - cm);
+      cm ^= b;
+      if ((lane >> k) & 1) {
+        const uint32_t m = __ffs(b) - 1;
+        sub |= b;
+        a1 += sm->xh1[m];
+        a2 += sm->xh2[m];
+      }
+    }
+    bool ok = lane != 0 && lane < (1u << ns);
+    cm = C;
+    #pragma unroll 1
+    for (uint32_t k = 0; k < ns; k++) {
+      const uint32_t b = cm & (0u - cm);
+      cm ^= b;
+      const uint32_t nbk = sm->xrow[__ffs(b) - 1];
+      // independent: no other member of the subset is a non-neighbour;
+      // maximal: every member outside has a non-neighbour inside
+      ok = ok && ((sub & b) ? (nbk & sub) == b : (nbk & sub) != 0);
+    }
+    const uint32_t mis = __ballot_sync(kFull, ok);
+    const uint32_t r = __popc(mis);
+    if (nent + r > 32) return false;
+    if (ok) {
+      const uint32_t e = nent + __popc(mis & lanemask_lt());
+      E1[e] = a1;
+      E2[e] = a2;
+      ES[e] = __popc(sub);
+    }
+    if (lane == j) {
+      c_off = nent;
+      c_r = r;
+    }
+    nent += r;
+    total *= r;
+  }
+  __syncwarp();
+  // the part every clique shares: R and the candidates adjacent to all others
+  const uint32_t base_cols = RM | single;
+  const uint64_t b1 = s10 + warp_sum_u64(((base_cols >> lane) & 1) ? t.h1 : 0);
+  const uint64_t b2 = s20 + warp_sum_u64(((base_cols >> lane) & 1) ? t.h2 : 0);
+  const uint32_t size0 = rsize0 + 2 + __popc(base_cols);
+  // sizes: the product of the components' size polynomials, lane = size - size0
+  // (a component's sets leave out at least one member, so sizes stay below size0 + 32)
+  uint32_t poly = lane == 0 ? 1u : 0u;
+  #pragma unroll 1
+  for (uint32_t j = 0; j < ncomp; j++) {
+    const uint32_t off = __shfl_sync(kFull, c_off, j), r = __shfl_sync(kFull, c_r, j);
+    uint32_t acc = 0;
+    #pragma unroll 1
+    for (uint32_t d = 0; d < r; d++) {
+      const uint32_t sz = ES[off + d];
+      const uint32_t v = __shfl_up_sync(kFull, poly, sz);
+      if (lane >= sz) acc += v;
+    }
+    poly = acc;
+  }
+  {
+    const uint32_t size = size0 + lane;
+    if (poly) {
+      if (size < kHistCache) {
+        atomicAdd(&sm->hcache[size], poly);
+      } else {
+        const EnumParams &Pm = *c.P;
+        const uint32_t bin = size < Pm.hist_len ? size : Pm.hist_len - 1;
+        atomicAdd(&Pm.hist[(uint64_t)sm->slot * Pm.hist_len + bin], (unsigned long long)poly);
+      }
+    }
+    const uint32_t mx = __reduce_max_sync(kFull, poly ? size : 0u);
+    if (lane == 0) {
+      sm->count += total;
+      sm->pending += (uint32_t)total;
+      sm->max_size = max(sm->max_size, mx);
+    }
+  }
+  // lane-carried components 0 .. a - 1 (Q products): each lane's own sums
+  uint32_t a = 0, Q = 1;
+  #pragma unroll 1
+  while (a < ncomp) {
+    const uint32_t r = __shfl_sync(kFull, c_r, a);
+    if (Q * r > 32) break;
+    Q *= r;
+    a++;
+  }
+  uint64_t p1 = b1, p2 = b2;
+  uint32_t psz = size0;
+  {
+    uint32_t rest = lane;
+    #pragma unroll 1
+    for (uint32_t j = 0; j < a; j++) {
+      const uint32_t off = __shfl_sync(kFull, c_off, j), r = __shfl_sync(kFull, c_r, j);
+      const uint32_t d = rest % r;
+      rest /= r;
+      p1 += E1[off + d];
+      p2 += E2[off + d];
+      psz += ES[off + d];
+    }
+  }
+  // counter-carried components a .. ncomp - 1: digits in lanes, sums uniform
+  uint32_t dig = 0;
+  uint64_t h1 = 0, h2 = 0;
+  uint32_t hsz = 0;
+  #pragma unroll 1
+  for (uint32_t j = a; j < ncomp; j++) {
+    const uint32_t off = __shfl_sync(kFull, c_off, j);
+    h1 += E1[off];
+    h2 += E2[off];
+    hsz += ES[off];
+  }
+  uint64_t chk = 0;
+  const bool live = lane < Q;
+  #pragma unroll 1
+  for (;;) {
+    if (live) chk += clique_hash(p1 + h1, p2 + h2, psz + hsz);
+    // next value of the counter: the lowest digit below its top moves up,
+    // the digits under it wrap to their first entry
+    const uint32_t can = __ballot_sync(kFull, lane >= a && lane < ncomp && dig + 1 < c_r);
+    if (!can) break;
+    const uint32_t jmax = __ffs(can) - 1;
+    #pragma unroll 1
+    for (uint32_t j = a; j <= jmax; j++) {
+      const uint32_t off = __shfl_sync(kFull, c_off, j);
+      const uint32_t cur = off + __shfl_sync(kFull, dig, j);
+      const uint32_t nxt = j == jmax ? cur + 1 : off;
+      h1 += E1[nxt] - E1[cur];
+      h2 += E2[nxt] - E2[cur];
+      hsz += ES[nxt] - ES[cur];
+    }
+    if (lane >= a && lane < jmax) dig = 0;
+    if (lane == jmax) dig++;
+  }
+  sm->lchk[lane] += chk;
+  __syncwarp();
+  maybe_flush(c);
+  return true;
+}
+
 // kStats: count search-tree nodes and row word-ops (a separate instance, so
 // the counting costs nothing when it is off)
 //
@@ -756,6 +967,7 @@ node:  // a node with candidates P, active rows A and R = RM
     t0_small(c, t, P, A, RM, npend, s10, s20, rsize0);
     goto backtrack;
   }
+  if (__popc(P) >= kJoinMin && (A & ~P) == 0 && t0_join(c, t, P, RM, s10, s20, rsize0)) goto backtrack;
   {
     const uint32_t key = (A & lanebit) ? (((uint32_t)__popc(P & ~t.row) << 5) | lane) : 0xffffffffu;
     const uint32_t kmin = __reduce_min_sync(kFull, key);

@@ -358,3 +358,74 @@ def test_batch_autotuner_recaptures(gpu, oracle_mod):
         b.close()
     for res, hist in outs[1:]:
         assert res == outs[0][0] and np.array_equal(hist, outs[0][1])
+
+
+def near_complete_blocks(seed, blocks=40, lo=12, hi=30, extra=6):
+    """Unions of near-complete blocks: each block is a clique minus the edges
+    of small complement components (perfect matchings, paths of three,
+    triangles, five-cycles), plus outside vertices adjacent to random parts of
+    a block (rows that hold R without being candidates).  Subproblems of such
+    blocks are exactly what the 32-bit tier's join decision takes, with and
+    without such rows."""
+    rng = np.random.default_rng(seed)
+    us, vs = [], []
+    base = 0
+    for _ in range(blocks):
+        b = int(rng.integers(lo, hi + 1))
+        verts = np.arange(base, base + b)
+        missing = set()
+        perm = rng.permutation(b)
+        i = 0
+        while i < b:
+            kind = int(rng.integers(0, 5))
+            comp = [int(x) for x in perm[i:i + (2, 3, 3, 5, 1)[kind]]]
+            i += len(comp)
+            if kind == 0 and len(comp) == 2:
+                missing.add((min(comp), max(comp)))
+            elif kind == 1:
+                for a, c in zip(comp, comp[1:]):
+                    missing.add((min(a, c), max(a, c)))
+            elif kind in (2, 3):
+                ring = comp + comp[:1] if len(comp) > 2 else comp
+                for a, c in zip(ring, ring[1:]):
+                    if a != c:
+                        missing.add((min(a, c), max(a, c)))
+        for a in range(b):
+            for c in range(a + 1, b):
+                if (a, c) not in missing:
+                    us.append(verts[a])
+                    vs.append(verts[c])
+        base += b
+        for _ in range(extra):
+            nbrs = verts[rng.random(b) < rng.uniform(0.3, 0.95)]
+            us.extend([base] * len(nbrs))
+            vs.extend(nbrs.tolist())
+            base += 1
+    # sparse links between blocks
+    for _ in range(blocks * 3):
+        a, c = rng.integers(0, base, 2)
+        if a != c:
+            us.append(a)
+            vs.append(c)
+    return np.array(us, np.uint32), np.array(vs, np.uint32)
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_near_complete_blocks(gpu, oracle_mod, seed):
+    u, v = near_complete_blocks(seed)
+    _, o = oracle_result(oracle_mod, u, v)
+    with gpu.Graph.from_coo(u, v, opts(gpu)) as g:
+        for kw in ({}, {"expand_r": 0}, {"flags": gpu.FLAG_NO_SHARING}):
+            r = g.solve(opts(gpu, **kw))
+            assert_same(r, o, f"seed {seed} {kw}")
+
+
+def test_cocktail_party(gpu, oracle_mod):
+    """K(2,2,...,2) on 28 vertices: 2^14 maximal cliques of 14 vertices."""
+    n = 28
+    u, v = zip(*[(a, c) for a in range(n) for c in range(a + 1, n) if c != a + 1 or a % 2])
+    u, v = np.array(u, np.uint32), np.array(v, np.uint32)
+    _, o = oracle_result(oracle_mod, u, v)
+    assert o.count == 2 ** 14 and o.hist == {14: 2 ** 14}
+    with gpu.Graph.from_coo(u, v, opts(gpu)) as g:
+        assert_same(g.solve(opts(gpu)), o, "cocktail party")

@@ -126,3 +126,43 @@ def test_subset_masks_match_direct_decision(n):
         rows = [sum(1 << k for k in range(n) if rnd.random() < 0.5) for _ in range(nrows)]
         holds = [sum(1 << r for r, row in enumerate(rows) if (row >> k) & 1) for k in range(n)]
         assert decide_by_masks(n, adj, holds) == decide_directly(n, adj, holds)
+
+
+def complement_components(g: nx.Graph, P):
+    h = nx.complement(g.subgraph(P))
+    return [sorted(c) for c in nx.connected_components(h)]
+
+
+def maximal_independent_sets(h: nx.Graph, comp):
+    out = []
+    for k in range(1, len(comp) + 1):
+        for s in itertools.combinations(comp, k):
+            ss = set(s)
+            if any(h.has_edge(x, y) for x, y in itertools.combinations(s, 2)):
+                continue
+            if any(not any(h.has_edge(w, x) for x in ss) for w in comp if w not in ss):
+                continue
+            out.append(ss)
+    return out
+
+
+@pytest.mark.parametrize("seed", range(20))
+def test_join_rule(seed):
+    """The 32-bit tier's join decision: when no vertex outside the candidates
+    is adjacent to all of R, the maximal cliques below are R + K for K the
+    products of one maximal independent set (in the complement H of G[P]) per
+    connected component of H."""
+    rnd = random.Random(1000 + seed)
+    n = rnd.randint(4, 13)
+    g = nx.complete_graph(n)
+    for _ in range(rnd.randint(0, n + 3)):
+        a, b = rnd.sample(range(n), 2)
+        if g.has_edge(a, b):
+            g.remove_edge(a, b)
+    P = list(range(n))
+    h = nx.complement(g.subgraph(P))
+    products = {frozenset()}
+    for comp in complement_components(g, P):
+        sets = maximal_independent_sets(h, comp)
+        products = {p | frozenset(s) for p in products for s in sets}
+    assert products == {frozenset(c) for c in nx.find_cliques(g)}
