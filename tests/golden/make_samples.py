@@ -84,7 +84,12 @@ def solve_record(g, roots, threads):
     cnt, chk, res = g.mce_root_set(roots, threads=threads)
     return {"roots": [int(r) for r in roots], "counts": [int(c) for c in cnt], "checksums": [f"{int(c):016x}" for c in chk],
             "count": int(res.count), "checksum": f"{res.checksum:016x}", "max_size": int(res.max_size),
-            "hist": {str(k): int(c) for k, c in sorted(res.hist.items())}, "oracle_seconds": round(time.time() - t, 1)}
+            "hist": {str(k): int(c) for k, c in sorted(res.hist.items())},
+            # the search tree of the reference's method (canonical pivot, EXPAND_R) over these roots: the
+            # algorithmic work the enumeration roofline is stated against
+            "canonical_tree": {"nodes": int(res.nodes), "pivot_words": int(res.pivot_words),
+                               "filter_rows": int(res.filter_rows), "build_bytes": int(res.build_bytes)},
+            "oracle_seconds": round(time.time() - t, 1)}
 
 
 def make_rmat20(threads):
