@@ -139,15 +139,35 @@ __global__ void __launch_bounds__(256) k_peel_rounds(uint32_t n, const uint32_t 
       ctl->rmin[(lev + 1) % 3] = 0xffffffffu;
     }
     uint32_t local_min = 0xffffffffu;
-    for (uint64_t i = tid; i < nrem; i += nthreads) {
-      const uint32_t v = __ldcg(rem_cur + i);
-      if (__ldcg(state + v)) continue;
-      const int d = __ldcg(deg + v);
-      if (d <= (int)k) {
+    // warp-uniform trip count; one atomic per warp and list (every survivor
+    // is appended at every level, so per-thread atomics on one counter would
+    // serialise)
+    for (uint64_t base = tid - lane; base < nrem; base += nthreads) {
+      const uint64_t i = base + lane;
+      uint32_t v = 0;
+      int d = 0;
+      bool claim = false, keep = false;
+      if (i < nrem) {
+        v = __ldcg(rem_cur + i);
+        if (!__ldcg(state + v)) {
+          d = __ldcg(deg + v);
+          claim = d <= (int)k;
+          keep = !claim;
+        }
+      }
+      const uint32_t cm = __ballot_sync(kFull, claim), km = __ballot_sync(kFull, keep);
+      uint32_t cb = 0, kb = 0;
+      if (lane == 0) {
+        if (cm) cb = atomicAdd(&ctl->fcnt[r % 3], (uint32_t)__popc(cm));
+        if (km) kb = atomicAdd(&ctl->rcnt[lev % 3], (uint32_t)__popc(km));
+      }
+      cb = __shfl_sync(kFull, cb, 0);
+      kb = __shfl_sync(kFull, kb, 0);
+      if (claim) {
         state[v] = r + 1;
-        fr[atomicAdd(&ctl->fcnt[r % 3], 1u)] = v;
-      } else {
-        rem_nxt[atomicAdd(&ctl->rcnt[lev % 3], 1u)] = v;
+        fr[cb + __popc(cm & lanemask_lt())] = v;
+      } else if (keep) {
+        rem_nxt[kb + __popc(km & lanemask_lt())] = v;
         local_min = min(local_min, (uint32_t)d);
       }
     }
@@ -163,10 +183,15 @@ __global__ void __launch_bounds__(256) k_peel_rounds(uint32_t n, const uint32_t 
       const uint32_t *cur = (r & 1) ? frB : frA;
       uint32_t *nxt = (r & 1) ? frA : frB;
       if (leader) ctl->fcnt[(r + 2) % 3] = 0;  // last read in round r - 1
-      for (uint64_t i = gwarp; i < nf; i += nwarps) {
+      // Each frontier vertex's adjacency is shared by `per` warps (all the
+      // grid's warps split evenly when the frontier is small: the dense
+      // cores' hubs hold tens of thousands of neighbours each).
+      const uint64_t per = nf < nwarps ? nwarps / nf : 1;
+      for (uint64_t i = gwarp / per; i < nf; i += nwarps / per) {
         const uint32_t v = __ldcg(cur + i);
         const uint32_t e1 = off[v + 1];
-        for (uint32_t e = off[v] + lane; e < e1; e += 32) {
+        const uint32_t part = (uint32_t)(gwarp % per);
+        for (uint64_t e = (uint64_t)off[v] + 32ULL * part + lane; e < e1; e += 32ULL * per) {
           const uint32_t u = adj[e];
           if (__ldcg(state + u)) continue;
           if (atomicSub(&deg[u], 1) == (int)k + 1 && atomicCAS(&state[u], 0u, r + 2) == 0u)
