@@ -360,6 +360,29 @@ def test_batch_autotuner_recaptures(gpu, oracle_mod):
         assert res == outs[0][0] and np.array_equal(hist, outs[0][1])
 
 
+def test_batch_options_take_effect(gpu, oracle_mod):
+    """A batch re-captures its launch when an option that feeds the plan
+    changes: a one-poll wait limit on the second solve must surface as
+    MCE_ERR_TIMEOUT (a stale capture would replay the first plan), and the
+    third solve, back on the defaults, must be exact again."""
+    graphs = [gpu.gen_batch_member(i)[:2] for i in range(200)]
+    want = []
+    for u, v in graphs[:20]:
+        want.append(oracle_mod.Graph.from_pairs(u, v).sort_degeneracy().mce(threads=4))
+    b = gpu.Batch(graphs, opts(gpu))
+    try:
+        first, _, _ = b.solve(opts(gpu, blocks_per_sm=4))
+        with pytest.raises(gpu.MceError) as e:
+            b.solve(gpu.options(blocks_per_sm=4, spin_limit=1))
+        assert e.value.status == gpu.ERR_TIMEOUT
+        third, _, _ = b.solve(opts(gpu, blocks_per_sm=4))
+    finally:
+        b.close()
+    assert third == first
+    for r, o in zip(third[:20], want):
+        assert (r["count"], r["checksum"], r["max_size"]) == (o.count, o.checksum, o.max_size)
+
+
 def near_complete_blocks(seed, blocks=40, lo=12, hi=30, extra=6):
     """Unions of near-complete blocks: each block is a clique minus the edges
     of small complement components (perfect matchings, paths of three,
