@@ -80,10 +80,11 @@ constexpr uint32_t kRegShareBound = 24;
 constexpr uint32_t kShareMin = 128, kShareMax = 8192;
 // 32-bit-tier nodes with this few candidates (5, 6 or 7) are decided in one
 // step.  Larger limits take more nodes off the search tree but grow the node
-// loop's code, and with the join decision below taking the large nodes, the
-// instruction cache is the tighter bound: 5 measured fastest.
+// loop's code (the instruction cache bounds the kernel): 6 measured as fast
+// as 5 where the join decision below takes most nodes, and 7 % faster where
+// it does not (active rows outside P); 7 was slower.
 #ifndef MCE_SMALL_P
-#define MCE_SMALL_P 5
+#define MCE_SMALL_P 6
 #endif
 constexpr int kSmallP = MCE_SMALL_P;
 static_assert(kSmallP >= 5 && kSmallP <= 7, "small-node decisions cover up to 5, 6 or 7 candidates");
